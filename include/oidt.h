@@ -1,0 +1,163 @@
+/*
+ * oidt.h -- C ABI of liboidt.so, the B200 (sm_100a) FDTD S-parameter engine.
+ *
+ * The reference runs one simulation per process: its fdtd_main.py builds the
+ * grid, copies every array to the device once
+ * (FDTD/GPU/FDTD_2D_TM/s-parameter_extraction/fdtd_main.py:216-261), launches
+ * 12 (2D) or 23 (3D) Numba kernels per time step (fdtd_main.py:275-304;
+ * FDTD/GPU/FDTD_3D/s-parameter_extraction/fdtd_main.py:357-406) and copies the
+ * port DFT accumulators back (fdtd_main.py:349-357).  This ABI replaces that
+ * device boundary with a job API: a job owns all device state of one
+ * simulation; host buffers are only borrowed for the duration of a call.
+ *
+ * Conventions
+ *  - Every function returns 0 (OIDT_OK) or a negative OIDT_ERR_* code; the
+ *    message is available from oidt_last_error(ctx).  No C++ exception
+ *    crosses this boundary.
+ *  - Arrays use the reference layout: 2D [nx][ny], 3D [nx][ny][nz], C order,
+ *    element type given by oidt_job_desc.precision.
+ *  - Field ids: OIDT_EX..OIDT_HZ.  2D TM uses EZ, HX, HY; 2D TE uses EX, EY,
+ *    HZ (the reference's fdtd_funcs.py kernels of each solver).
+ *  - Waits are bounded: oidt_job_sync returns OIDT_ERR_TIMEOUT after
+ *    timeout_ms instead of blocking forever.
+ */
+#ifndef OIDT_H
+#define OIDT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OIDT_ABI_VERSION 1
+
+/* status codes */
+#define OIDT_OK 0
+#define OIDT_ERR_INVALID (-1)  /* bad argument or descriptor            */
+#define OIDT_ERR_CUDA (-2)     /* CUDA runtime error                      */
+#define OIDT_ERR_BUDGET (-3)   /* admission would exceed the HBM budget   */
+#define OIDT_ERR_NOTFOUND (-4) /* unknown job id                          */
+#define OIDT_ERR_TIMEOUT (-5)  /* bounded wait expired                    */
+#define OIDT_ERR_STATE (-6)    /* call not valid in the job's state       */
+
+/* solvers: the three reference directories FDTD/GPU/FDTD_{2D_TM,2D_TE,3D} */
+#define OIDT_MODE_TM2 0
+#define OIDT_MODE_TE2 1
+#define OIDT_MODE_YEE3D 2
+
+#define OIDT_F32 0
+#define OIDT_F64 1
+
+/* OIDT_ARITH_FAST: reciprocal multiplies and fused multiply-adds.
+ * OIDT_ARITH_EXACT: the reference's operation order with IEEE divisions and
+ * no contraction, so a float64 run reproduces the reference's float64 run
+ * bit for bit. */
+#define OIDT_ARITH_FAST 0
+#define OIDT_ARITH_EXACT 1
+
+#define OIDT_EX 0
+#define OIDT_EY 1
+#define OIDT_EZ 2
+#define OIDT_HX 3
+#define OIDT_HY 4
+#define OIDT_HZ 5
+
+typedef struct oidt_ctx oidt_ctx;
+
+/* One simulation.  Mirrors the arrays and scalars the reference passes to
+ * its kernels (fdtd_main.py:216-261, 3D :258-343). */
+typedef struct oidt_job_desc {
+  int32_t mode;      /* OIDT_MODE_*                                        */
+  int32_t precision; /* OIDT_F32 / OIDT_F64: fields, coefficients, psi     */
+  int32_t arith;     /* OIDT_ARITH_*                                       */
+  int32_t nx, ny, nz;/* nz = 1 in 2D                                       */
+  int32_t num_cpml;  /* P                                                  */
+  int32_t ib, jb, kb, ie, je, ke; /* update limits (reference offset = 2)  */
+  int32_t nt;        /* steps covered by j_src and the twiddle tables      */
+  int32_t nf;        /* DFT frequencies                                    */
+  /* E-component update coefficients dt/eps, full grids:
+   * TM2 {CBZ}, TE2 {CBX, CBY}, 3D {CBX, CBY, CBZ}; unused entries NULL */
+  const void *cb[3];
+  /* kappa*dx divisors: kxe, kye, kze, kxh, kyh, kzh (length nx, ny, nz);
+   * 2D: kze = kzh = NULL */
+  const void *kdx[6];
+  const void *be, *ce, *bh, *ch; /* CPML recursion coefficients [P]        */
+  double db;         /* dt/mu, cast to precision                           */
+  double dx;         /* the divisor the CPML kernels use                   */
+  /* soft source: field[src_lo..src_hi) -= j_src[n] each step              */
+  int32_t src_field;
+  int32_t src_lo[3], src_hi[3];
+  const void *j_src; /* [nt]                                               */
+  /* port DFT planes: 2D x = port_pos[q], window j in [win_lo[1], win_hi[1]);
+   * 3D z = port_pos[q], window i in [win_lo[0], win_hi[0]), j in
+   * [win_lo[1], win_hi[1]) */
+  int32_t port_pos[2];
+  int32_t win_lo[2], win_hi[2];
+  /* float64 twiddles [nf][nt]: cos/sin(2 pi f n dt) and at (n + 1/2) dt */
+  const double *cos_e, *sin_e, *cos_h, *sin_h;
+  int32_t ring_steps; /* steps buffered between DFT folds (0 = default)    */
+  int32_t reserved[7];
+} oidt_job_desc;
+
+typedef struct oidt_stats {
+  uint64_t hbm_budget;   /* admission budget in bytes                      */
+  uint64_t hbm_in_use;   /* bytes held by live jobs                        */
+  int32_t live_jobs;
+  int32_t device;
+  int64_t kernel_launches; /* kernels this context has launched            */
+} oidt_stats;
+
+int32_t oidt_abi_version(void);
+
+/* Context: one per device.  hbm_budget = 0 means 90 % of free memory. */
+int32_t oidt_create(int32_t device, uint64_t hbm_budget, oidt_ctx **out);
+int32_t oidt_destroy(oidt_ctx *ctx);
+const char *oidt_last_error(oidt_ctx *ctx);
+int32_t oidt_stats_get(oidt_ctx *ctx, oidt_stats *out);
+
+/* Device bytes a job with this descriptor would hold (admission check). */
+int32_t oidt_job_bytes(const oidt_job_desc *desc, uint64_t *bytes);
+
+/* Allocate device state, copy the descriptor's host arrays (H2D), zero the
+ * fields, psi and DFT accumulators.  Replaces fdtd_main.py:51-261. */
+int32_t oidt_job_create(oidt_ctx *ctx, const oidt_job_desc *desc, uint64_t *job);
+
+/* Enqueue nsteps time steps (asynchronous).  Replaces the hot loop
+ * fdtd_main.py:275-304 (3D :357-406); the DFT fold runs every ring_steps
+ * steps and at the end of the call. */
+int32_t oidt_job_advance(oidt_ctx *ctx, uint64_t job, int32_t nsteps);
+
+/* Advance several jobs together: one multi-instance launch per half step
+ * over all the jobs' tiles (jobs may differ in size and solver). */
+int32_t oidt_batch_advance(oidt_ctx *ctx, const uint64_t *jobs, int32_t njobs, int32_t nsteps);
+
+/* Bounded wait for the job's enqueued work.  timeout_ms < 0: no limit. */
+int32_t oidt_job_sync(oidt_ctx *ctx, uint64_t job, int32_t timeout_ms);
+
+/* Steps completed so far (after a sync) and whether work is in flight. */
+int32_t oidt_job_query(oidt_ctx *ctx, uint64_t job, int32_t *steps_done, int32_t *busy);
+
+/* Port DFT of one component as complex128 (re, im interleaved), reference
+ * layout: 2D [nf][ny], 3D [nf][nx][ny], zero outside the window.
+ * comp: 2D 0 = E (Ez TM / Ey TE), 1 = H (Hy TM / Hz TE);
+ *       3D 0 = Ex, 1 = Ey, 2 = Hx, 3 = Hy.  Replaces fdtd_main.py:349-363. */
+int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t comp,
+                          double *out_re_im, size_t n_doubles);
+
+/* Field snapshot / overwrite (reference layout, job precision). */
+int32_t oidt_job_read_field(oidt_ctx *ctx, uint64_t job, int32_t field, void *out, size_t nbytes);
+int32_t oidt_job_write_field(oidt_ctx *ctx, uint64_t job, int32_t field, const void *src, size_t nbytes);
+
+/* CPML auxiliary array of field `field` for slab axis `axis` (0 x, 1 y, 2 z)
+ * and side (0 low, 1 high), in the reference's PSI_<F>_<A><LO|HI> layout. */
+int32_t oidt_job_read_psi(oidt_ctx *ctx, uint64_t job, int32_t field, int32_t axis, int32_t side,
+                          void *out, size_t nbytes);
+
+int32_t oidt_job_release(oidt_ctx *ctx, uint64_t job);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OIDT_H */

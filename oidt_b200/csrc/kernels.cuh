@@ -1,0 +1,432 @@
+// kernels.cuh -- per-cell Yee updates for the three reference solvers, with
+// the CPML psi recursion, the soft source and the port-plane capture fused in.
+//
+// One thread owns one cell and applies, for each field component it updates,
+// exactly the sequence of operations the reference applies to that cell in
+// one time step: curl update, source, then the CPML corrections in the
+// reference's launch order.  With Ar<T, true> (OIDT_ARITH_EXACT) every
+// operation is an IEEE add/sub/mul/div in the reference's operand order, so
+// float64 results equal the reference's float64 results bit for bit.
+//
+// Reference kernels restated here:
+//   TM2  FDTD/GPU/FDTD_2D_TM/s-parameter_extraction/fdtd_funcs.py:43-124
+//   TE2  FDTD/GPU/FDTD_2D_TE/s-parameter_extraction/fdtd_funcs.py:43-124
+//   3D   FDTD/GPU/FDTD_3D/s-parameter_extraction/fdtd_funcs.py:43-266
+// and the per-step launch order of fdtd_main.py:275-304 (3D :357-406).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace oidt {
+
+enum { EX = 0, EY = 1, EZ = 2, HX = 3, HY = 4, HZ = 5 };
+enum { AX = 0, AY = 1, AZ = 2 };
+enum { LO = 0, HI = 1 };
+
+// ---------------------------------------------------------------------------
+// Arithmetic policy.
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT> struct Ar;
+template <> struct Ar<float, true> {
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b, float) { return __fdiv_rn(a, b); }
+};
+template <> struct Ar<float, false> {
+  static __device__ __forceinline__ float add(float a, float b) { return a + b; }
+  static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+  static __device__ __forceinline__ float mul(float a, float b) { return a * b; }
+  static __device__ __forceinline__ float div(float a, float, float rb) { return a * rb; }
+};
+template <> struct Ar<double, true> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b, double) { return __ddiv_rn(a, b); }
+};
+template <> struct Ar<double, false> {
+  static __device__ __forceinline__ double add(double a, double b) { return a + b; }
+  static __device__ __forceinline__ double sub(double a, double b) { return a - b; }
+  static __device__ __forceinline__ double mul(double a, double b) { return a * b; }
+  static __device__ __forceinline__ double div(double a, double, double rb) { return a * rb; }
+};
+
+// ---------------------------------------------------------------------------
+// Job parameters (device-resident copy for batched launches).
+// ---------------------------------------------------------------------------
+template <typename T> struct Params {
+  int mode;              // OIDT_MODE_*
+  int nx, ny, nz;        // nz = 1 in 2D
+  int P, ib, jb, kb, ie, je, ke;
+  T *f[6];               // fields, reference layout
+  const T *cb[3];        // dt/eps per E component (TM2 uses cb[2] for Ez)
+  const T *kd[6];        // kappa*dx: kxe kye kze kxh kyh kzh
+  const T *rkd[6];       // reciprocals
+  const T *be, *ce, *bh, *ch;
+  T db, dx, rdx;
+  T *psi[6][3][2];       // [field][slab axis][side]
+  int src_field;         // -1: none
+  int slo[3], shi[3];
+  const T *jsrc;
+  T *ring;               // capture ring [K][2 ports][slots][plane]
+  int ring_K, nslot;
+  long long plane;       // 2D: ny, 3D: nx*ny
+  int port_pos[2];
+  int *state;            // state[0] = absolute step of ring slot 0
+};
+
+template <typename T>
+__device__ __forceinline__ bool in_src(const Params<T> &p, int fld, int i, int j, int k) {
+  return p.src_field == fld && i >= p.slo[0] && i < p.shi[0] && j >= p.slo[1] && j < p.shi[1] &&
+         k >= p.slo[2] && k < p.shi[2];
+}
+
+// psi array index for a 3D slab array whose `axis` extent is P.
+__device__ __forceinline__ long long psi_idx3(int axis, int i, int j, int k, int nx, int ny, int nz,
+                                              int P) {
+  if (axis == AX) return ((long long)i * ny + j) * nz + k;  // i is the slab index d
+  if (axis == AY) return ((long long)i * P + j) * nz + k;   // j is d
+  return ((long long)i * ny + j) * P + k;                   // k is d
+}
+
+// E-field CPML slab test along one axis: returns coefficient index or -1,
+// writes slab index d and side.  Low slab cells b..b+P-1 (coef P-1-d), high
+// slab cells e-P..e-1 (coef d).  (fdtd_funcs.py update_pml_e*: be[-(d+1)],
+// be[d].)
+__device__ __forceinline__ int e_slab(int c, int b, int e, int P, int &d, int &side) {
+  if (c >= b && c < b + P) { d = c - b; side = LO; return P - 1 - d; }
+  if (c >= e - P && c < e) { d = c - (e - P); side = HI; return d; }
+  return -1;
+}
+// H-field CPML slab: low cells b+1..b+P-1 (coef P-d), high e-P+1..e-1 (coef
+// d), d in 1..P-1.  (update_pml_h*: ``i > 0 and i < pmle``, bh[-d], bh[d].)
+__device__ __forceinline__ int h_slab(int c, int b, int e, int P, int &d, int &side) {
+  if (c > b && c < b + P) { d = c - b; side = LO; return P - d; }
+  if (c > e - P && c < e) { d = c - (e - P); side = HI; return d; }
+  return -1;
+}
+
+template <typename T>
+__device__ __forceinline__ void capture(const Params<T> &p, int s, int port, int slot, long long idx,
+                                        T v) {
+  p.ring[(((long long)s * 2 + port) * p.nslot + slot) * p.plane + idx] = v;
+}
+
+// ---------------------------------------------------------------------------
+// 3D Yee (FDTD/GPU/FDTD_3D/s-parameter_extraction/fdtd_funcs.py)
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT>
+__device__ __forceinline__ void y3_e_cell(const Params<T> &p, int i, int j, int k, int n, int s) {
+  using A = Ar<T, EXACT>;
+  const int nx = p.nx, ny = p.ny, nz = p.nz, P = p.P;
+  const long long sy = nz, sx = (long long)ny * nz;
+  const long long c = i * sx + j * sy + k;
+  const T *Hx = p.f[HX], *Hy = p.f[HY], *Hz = p.f[HZ];
+  const T Jn = p.src_field >= 0 ? p.jsrc[n] : T(0);
+  int d, side, q;
+  // Ex: i in (ib, ie), j in [jb, je), k in [kb, ke)         :43-50
+  if (i > p.ib && i < p.ie && j >= p.jb && j < p.je && k >= p.kb && k < p.ke) {
+    const T cb = p.cb[0][c];
+    const T dhz = A::sub(Hz[c + sy], Hz[c]);
+    const T dhy = A::sub(Hy[c + 1], Hy[c]);
+    T e = A::add(p.f[EX][c], A::mul(cb, A::sub(A::div(dhz, p.kd[1][j], p.rkd[1][j]),
+                                                A::div(dhy, p.kd[2][k], p.rkd[2][k]))));
+    if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc :113-123
+      T *ps = p.psi[EX][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
+      *ps = v;
+      e = A::add(e, A::mul(cb, v));
+    }
+    if ((q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ex_zinc :126-136
+      T hy1 = Hy[c + 1], hy0 = Hy[c];
+      if (p.src_field == HY) {  // the Hy source lands between the E curl and E-CPML
+        if (in_src(p, HY, i, j, k + 1)) hy1 = A::sub(hy1, Jn);
+        if (in_src(p, HY, i, j, k)) hy0 = A::sub(hy0, Jn);
+      }
+      T *ps = p.psi[EX][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], A::sub(hy1, hy0)), p.dx, p.rdx));
+      *ps = v;
+      e = A::sub(e, A::mul(cb, v));
+    }
+    p.f[EX][c] = e;
+    if (k == p.port_pos[0]) capture(p, s, 0, 0, (long long)i * ny + j, e);
+    if (k == p.port_pos[1]) capture(p, s, 1, 0, (long long)i * ny + j, e);
+  }
+  // Ey: i in [ib, ie), j in (jb, je), k in [kb, ke)         :53-60
+  if (i >= p.ib && i < p.ie && j > p.jb && j < p.je && k >= p.kb && k < p.ke) {
+    const T cb = p.cb[1][c];
+    const T dhx = A::sub(Hx[c + 1], Hx[c]);
+    const T dhz = A::sub(Hz[c + sx], Hz[c]);
+    T e = A::add(p.f[EY][c], A::mul(cb, A::sub(A::div(dhx, p.kd[2][k], p.rkd[2][k]),
+                                                A::div(dhz, p.kd[0][i], p.rkd[0][i]))));
+    if (in_src(p, EY, i, j, k)) e = A::sub(e, Jn);       // update_source :104-110
+    if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc :139-149
+      T *ps = p.psi[EY][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
+      *ps = v;
+      e = A::sub(e, A::mul(cb, v));
+    }
+    if ((q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ey_zinc :152-162
+      T *ps = p.psi[EY][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
+      *ps = v;
+      e = A::add(e, A::mul(cb, v));
+    }
+    p.f[EY][c] = e;
+    if (k == p.port_pos[0]) capture(p, s, 0, 1, (long long)i * ny + j, e);
+    if (k == p.port_pos[1]) capture(p, s, 1, 1, (long long)i * ny + j, e);
+  }
+  // Ez: i in [ib, ie), j in [jb, je), k in (kb, ke)         :63-70
+  if (i >= p.ib && i < p.ie && j >= p.jb && j < p.je && k > p.kb && k < p.ke) {
+    const T cb = p.cb[2][c];
+    const T dhy = A::sub(Hy[c + sx], Hy[c]);
+    const T dhx = A::sub(Hx[c + sy], Hx[c]);
+    T e = A::add(p.f[EZ][c], A::mul(cb, A::sub(A::div(dhy, p.kd[0][i], p.rkd[0][i]),
+                                                A::div(dhx, p.kd[1][j], p.rkd[1][j]))));
+    if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ez_xinc :165-175
+      T hy1 = Hy[c + sx], hy0 = Hy[c];
+      if (p.src_field == HY) {
+        if (in_src(p, HY, i + 1, j, k)) hy1 = A::sub(hy1, Jn);
+        if (in_src(p, HY, i, j, k)) hy0 = A::sub(hy0, Jn);
+      }
+      T *ps = p.psi[EZ][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], A::sub(hy1, hy0)), p.dx, p.rdx));
+      *ps = v;
+      e = A::add(e, A::mul(cb, v));
+    }
+    if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ez_yinc :178-188
+      T *ps = p.psi[EZ][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
+      *ps = v;
+      e = A::sub(e, A::mul(cb, v));
+    }
+    p.f[EZ][c] = e;
+  }
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int k, int n, int s) {
+  using A = Ar<T, EXACT>;
+  const int nx = p.nx, ny = p.ny, nz = p.nz, P = p.P;
+  const long long sy = nz, sx = (long long)ny * nz;
+  const long long c = i * sx + j * sy + k;
+  const T *Ex = p.f[EX], *Ey = p.f[EY], *Ez = p.f[EZ];
+  const T db = p.db;
+  int d, side, q;
+  // Hx: i in [ib, ie), j in (jb, je), k in (kb, ke)         :73-80
+  if (i >= p.ib && i < p.ie && j > p.jb && j < p.je && k > p.kb && k < p.ke) {
+    const T dey = A::sub(Ey[c], Ey[c - 1]);
+    const T dez = A::sub(Ez[c], Ez[c - sy]);
+    T h = A::add(p.f[HX][c], A::mul(db, A::sub(A::div(dey, p.kd[5][k], p.rkd[5][k]),
+                                                A::div(dez, p.kd[4][j], p.rkd[4][j]))));
+    if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc :191-201
+      T *ps = p.psi[HX][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
+      *ps = v;
+      h = A::sub(h, A::mul(db, v));
+    }
+    if ((q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hx_zinc :204-214
+      T *ps = p.psi[HX][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
+      *ps = v;
+      h = A::add(h, A::mul(db, v));
+    }
+    p.f[HX][c] = h;
+    if (k == p.port_pos[0]) capture(p, s, 0, 2, (long long)i * ny + j, h);
+    if (k == p.port_pos[1]) capture(p, s, 1, 2, (long long)i * ny + j, h);
+    if (k == p.port_pos[0] + 1) capture(p, s, 0, 3, (long long)i * ny + j, h);
+    if (k == p.port_pos[1] + 1) capture(p, s, 1, 3, (long long)i * ny + j, h);
+  }
+  // Hy: i in (ib, ie), j in [jb, je), k in (kb, ke)         :83-90
+  if (i > p.ib && i < p.ie && j >= p.jb && j < p.je && k > p.kb && k < p.ke) {
+    const T dez = A::sub(Ez[c], Ez[c - sx]);
+    const T dex = A::sub(Ex[c], Ex[c - 1]);
+    T h = p.f[HY][c];
+    if (in_src(p, HY, i, j, k)) h = A::sub(h, p.jsrc[n]);  // source precedes update_hy
+    h = A::add(h, A::mul(db, A::sub(A::div(dez, p.kd[3][i], p.rkd[3][i]),
+                                     A::div(dex, p.kd[5][k], p.rkd[5][k]))));
+    if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hy_xinc :217-227
+      T *ps = p.psi[HY][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
+      *ps = v;
+      h = A::add(h, A::mul(db, v));
+    }
+    if ((q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hy_zinc :230-240
+      T *ps = p.psi[HY][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
+      *ps = v;
+      h = A::sub(h, A::mul(db, v));
+    }
+    p.f[HY][c] = h;
+    if (k == p.port_pos[0]) capture(p, s, 0, 4, (long long)i * ny + j, h);
+    if (k == p.port_pos[1]) capture(p, s, 1, 4, (long long)i * ny + j, h);
+    if (k == p.port_pos[0] + 1) capture(p, s, 0, 5, (long long)i * ny + j, h);
+    if (k == p.port_pos[1] + 1) capture(p, s, 1, 5, (long long)i * ny + j, h);
+  }
+  // Hz: i in (ib, ie), j in (jb, je), k in [kb, ke)         :93-100
+  if (i > p.ib && i < p.ie && j > p.jb && j < p.je && k >= p.kb && k < p.ke) {
+    const T dex = A::sub(Ex[c], Ex[c - sy]);
+    const T dey = A::sub(Ey[c], Ey[c - sx]);
+    T h = A::add(p.f[HZ][c], A::mul(db, A::sub(A::div(dex, p.kd[4][j], p.rkd[4][j]),
+                                                A::div(dey, p.kd[3][i], p.rkd[3][i]))));
+    if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hz_xinc :243-253
+      T *ps = p.psi[HZ][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
+      *ps = v;
+      h = A::sub(h, A::mul(db, v));
+    }
+    if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hz_yinc :256-266
+      T *ps = p.psi[HZ][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
+      *ps = v;
+      h = A::add(h, A::mul(db, v));
+    }
+    p.f[HZ][c] = h;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2D TM (FDTD/GPU/FDTD_2D_TM/s-parameter_extraction/fdtd_funcs.py)
+// psi arrays: x-slab [P][ny], y-slab [nx][P].
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT>
+__device__ __forceinline__ void tm2_e_cell(const Params<T> &p, int i, int j, int n, int s) {
+  using A = Ar<T, EXACT>;
+  const int ny = p.ny, P = p.P;
+  const long long c = (long long)i * ny + j;
+  const T *Hx = p.f[HX], *Hy = p.f[HY];
+  int d, side, q;
+  if (i >= p.ib && i < p.ie && j >= p.jb && j < p.je) {  // update_ez :44-49
+    const T cb = p.cb[2][c];
+    const T dhy = A::sub(Hy[c + ny], Hy[c]);
+    const T dhx = A::sub(Hx[c + 1], Hx[c]);
+    T e = A::add(p.f[EZ][c], A::mul(cb, A::sub(A::div(dhy, p.kd[0][i], p.rkd[0][i]),
+                                                A::div(dhx, p.kd[1][j], p.rkd[1][j]))));
+    if (in_src(p, EZ, i, j, 0)) e = A::sub(e, p.jsrc[n]);  // update_source :71-76
+    if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {    // update_pml_ez_xinc :80-88
+      T *ps = p.psi[EZ][AX][side] + (long long)d * ny + j;
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhy), p.dx, p.rdx));
+      *ps = v;
+      e = A::add(e, A::mul(cb, v));
+    }
+    if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {    // update_pml_ez_yinc :92-100
+      T *ps = p.psi[EZ][AY][side] + (long long)i * P + d;
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
+      *ps = v;
+      e = A::sub(e, A::mul(cb, v));
+    }
+    p.f[EZ][c] = e;
+    if (i == p.port_pos[0]) capture(p, s, 0, 0, j, e);
+    if (i == p.port_pos[1]) capture(p, s, 1, 0, j, e);
+  }
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void tm2_h_cell(const Params<T> &p, int i, int j, int n, int s) {
+  using A = Ar<T, EXACT>;
+  const int ny = p.ny, P = p.P;
+  const long long c = (long long)i * ny + j;
+  const T *Ez = p.f[EZ];
+  const T db = p.db;
+  int d, side, q;
+  if (i >= p.ib && i < p.ie && j > p.jb && j < p.je) {  // update_hx :53-58
+    const T dez = A::sub(Ez[c - 1], Ez[c]);
+    T h = A::add(p.f[HX][c], A::div(A::mul(db, dez), p.kd[4][j], p.rkd[4][j]));
+    if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {   // update_pml_hx_yinc :104-112
+      T *ps = p.psi[HX][AY][side] + (long long)i * P + d;
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], A::sub(Ez[c], Ez[c - 1])), p.dx, p.rdx));
+      *ps = v;
+      h = A::sub(h, A::mul(db, v));
+    }
+    p.f[HX][c] = h;
+  }
+  if (i > p.ib && i < p.ie && j >= p.jb && j < p.je) {  // update_hy :62-67
+    const T dez = A::sub(Ez[c], Ez[c - ny]);
+    T h = A::add(p.f[HY][c], A::div(A::mul(db, dez), p.kd[3][i], p.rkd[3][i]));
+    if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {   // update_pml_hy_xinc :116-124
+      T *ps = p.psi[HY][AX][side] + (long long)d * ny + j;
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
+      *ps = v;
+      h = A::add(h, A::mul(db, v));
+    }
+    p.f[HY][c] = h;
+    if (i == p.port_pos[0]) capture(p, s, 0, 1, j, h);
+    if (i == p.port_pos[1]) capture(p, s, 1, 1, j, h);
+    if (i == p.port_pos[0] + 1) capture(p, s, 0, 2, j, h);
+    if (i == p.port_pos[1] + 1) capture(p, s, 1, 2, j, h);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2D TE (FDTD/GPU/FDTD_2D_TE/s-parameter_extraction/fdtd_funcs.py)
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT>
+__device__ __forceinline__ void te2_e_cell(const Params<T> &p, int i, int j, int n, int s) {
+  using A = Ar<T, EXACT>;
+  const int ny = p.ny, P = p.P;
+  const long long c = (long long)i * ny + j;
+  const T *Hz = p.f[HZ];
+  int d, side, q;
+  if (i > p.ib && i < p.ie && j >= p.jb && j < p.je) {  // update_ex :43-49
+    const T cb = p.cb[0][c];
+    const T dhz = A::sub(Hz[c + 1], Hz[c]);
+    T e = A::add(p.f[EX][c], A::div(A::mul(cb, dhz), p.kd[1][j], p.rkd[1][j]));
+    if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {   // update_pml_ex_yinc :79-87
+      T *ps = p.psi[EX][AY][side] + (long long)i * P + d;
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
+      *ps = v;
+      e = A::add(e, A::mul(cb, v));
+    }
+    p.f[EX][c] = e;
+  }
+  if (i >= p.ib && i < p.ie && j > p.jb && j < p.je) {  // update_ey :52-58
+    const T cb = p.cb[1][c];
+    T e = A::add(p.f[EY][c], A::div(A::mul(cb, A::sub(Hz[c], Hz[c + ny])), p.kd[0][i], p.rkd[0][i]));
+    if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {   // update_pml_ey_xinc :91-99
+      T *ps = p.psi[EY][AX][side] + (long long)d * ny + j;
+      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], A::sub(Hz[c + ny], Hz[c])), p.dx, p.rdx));
+      *ps = v;
+      e = A::sub(e, A::mul(cb, v));
+    }
+    p.f[EY][c] = e;
+    if (i == p.port_pos[0]) capture(p, s, 0, 0, j, e);
+    if (i == p.port_pos[1]) capture(p, s, 1, 0, j, e);
+  }
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void te2_h_cell(const Params<T> &p, int i, int j, int n, int s) {
+  using A = Ar<T, EXACT>;
+  const int ny = p.ny, P = p.P;
+  const long long c = (long long)i * ny + j;
+  const T *Ex = p.f[EX], *Ey = p.f[EY];
+  const T db = p.db;
+  int d, side, q;
+  if (i > p.ib && i < p.ie && j > p.jb && j < p.je) {  // update_hz :61-67
+    const T dex = A::sub(Ex[c], Ex[c - 1]);
+    const T dey = A::sub(Ey[c], Ey[c - ny]);
+    T h = A::add(p.f[HZ][c], A::mul(db, A::sub(A::div(dex, p.kd[4][j], p.rkd[4][j]),
+                                                A::div(dey, p.kd[3][i], p.rkd[3][i]))));
+    if (in_src(p, HZ, i, j, 0)) h = A::sub(h, p.jsrc[n]);  // source after update_hz
+    if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {     // update_pml_hz_xinc :103-111
+      T *ps = p.psi[HZ][AX][side] + (long long)d * ny + j;
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
+      *ps = v;
+      h = A::sub(h, A::mul(db, v));
+    }
+    if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {     // update_pml_hz_yinc :115-123
+      T *ps = p.psi[HZ][AY][side] + (long long)i * P + d;
+      T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
+      *ps = v;
+      h = A::add(h, A::mul(db, v));
+    }
+    p.f[HZ][c] = h;
+    if (i == p.port_pos[0]) capture(p, s, 0, 1, j, h);
+    if (i == p.port_pos[1]) capture(p, s, 1, 1, j, h);
+    if (i == p.port_pos[0] + 1) capture(p, s, 0, 2, j, h);
+    if (i == p.port_pos[1] + 1) capture(p, s, 1, 2, j, h);
+  }
+}
+
+}  // namespace oidt

@@ -1,0 +1,207 @@
+"""Python binding of ``liboidt.so`` (ctypes) and the job wrapper.
+
+The library is built in-tree (``oidt_b200/liboidt.so``, see ``build.py``).
+Importing this module on a machine without the library raises: there is no
+CPU fallback for the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+from .spec import DFT_COMPS, FIELD_ID, FIELDS, PSI, SimSpec, to_desc
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboidt.so")
+
+OK, ERR_INVALID, ERR_CUDA, ERR_BUDGET, ERR_NOTFOUND, ERR_TIMEOUT, ERR_STATE = 0, -1, -2, -3, -4, -5, -6
+EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error", "oidt_stats_get",
+           "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
+           "oidt_job_query", "oidt_job_read_dft", "oidt_job_read_field", "oidt_job_write_field",
+           "oidt_job_read_psi", "oidt_job_release")
+
+
+class OidtError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("oidt error %d: %s" % (code, msg))
+        self.code = code
+
+
+class BudgetError(OidtError):
+    pass
+
+
+class TimeoutError_(OidtError):
+    pass
+
+
+class Stats(C.Structure):
+    _fields_ = [("hbm_budget", C.c_uint64), ("hbm_in_use", C.c_uint64), ("live_jobs", C.c_int32),
+                ("device", C.c_int32), ("kernel_launches", C.c_int64)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load_library(path: str = LIB_PATH):
+    """Load (once) and type the C ABI.  Raises if the library is missing."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(path):
+            raise ImportError("liboidt.so not found at %s; run `python -m oidt_b200.build`" % path)
+        L = C.CDLL(path)
+        vp, u64, i32 = C.c_void_p, C.c_uint64, C.c_int32
+        sig = {
+            "oidt_abi_version": ([], i32),
+            "oidt_create": ([i32, u64, C.POINTER(vp)], i32),
+            "oidt_destroy": ([vp], i32),
+            "oidt_last_error": ([vp], C.c_char_p),
+            "oidt_stats_get": ([vp, C.POINTER(Stats)], i32),
+            "oidt_job_bytes": ([vp, C.POINTER(u64)], i32),
+            "oidt_job_create": ([vp, vp, C.POINTER(u64)], i32),
+            "oidt_job_advance": ([vp, u64, i32], i32),
+            "oidt_batch_advance": ([vp, C.POINTER(u64), i32, i32], i32),
+            "oidt_job_sync": ([vp, u64, i32], i32),
+            "oidt_job_query": ([vp, u64, C.POINTER(i32), C.POINTER(i32)], i32),
+            "oidt_job_read_dft": ([vp, u64, i32, i32, vp, C.c_size_t], i32),
+            "oidt_job_read_field": ([vp, u64, i32, vp, C.c_size_t], i32),
+            "oidt_job_write_field": ([vp, u64, i32, vp, C.c_size_t], i32),
+            "oidt_job_read_psi": ([vp, u64, i32, i32, i32, vp, C.c_size_t], i32),
+            "oidt_job_release": ([vp, u64], i32),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+        return L
+
+
+class Engine:
+    """One context on one device (``oidt_create``)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.lib = load_library()
+        self.ctx = C.c_void_p()
+        rc = self.lib.oidt_create(device, hbm_budget, C.byref(self.ctx))
+        if rc != OK:
+            raise OidtError(rc, "oidt_create(device=%d) failed (no usable CUDA device?)" % device)
+        self.device = device
+
+    def _check(self, rc):
+        if rc == OK:
+            return
+        msg = self.lib.oidt_last_error(self.ctx).decode()
+        if rc == ERR_BUDGET:
+            raise BudgetError(rc, msg)
+        if rc == ERR_TIMEOUT:
+            raise TimeoutError_(rc, msg)
+        raise OidtError(rc, msg)
+
+    def close(self):
+        if self.ctx:
+            self.lib.oidt_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self.lib.oidt_stats_get(self.ctx, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def job_bytes(self, spec: SimSpec, precision=None, ring_steps=0) -> int:
+        d, keep = to_desc(spec, precision=precision, ring_steps=ring_steps)
+        b = C.c_uint64()
+        self._check(self.lib.oidt_job_bytes(C.byref(d), C.byref(b)))
+        return b.value
+
+    def submit(self, spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0) -> "Job":
+        d, keep = to_desc(spec, arith=arith, precision=precision, ring_steps=ring_steps)
+        jid = C.c_uint64()
+        self._check(self.lib.oidt_job_create(self.ctx, C.byref(d), C.byref(jid)))
+        del keep
+        return Job(self, jid.value, spec, np.dtype(precision if precision is not None else spec.precision))
+
+    def batch_advance(self, jobs, nsteps: int):
+        ids = (C.c_uint64 * len(jobs))(*[j.id for j in jobs])
+        self._check(self.lib.oidt_batch_advance(self.ctx, ids, len(jobs), nsteps))
+        for j in jobs:
+            j.steps += nsteps
+
+
+class Job:
+    """One simulation's device state (``oidt_job_*``)."""
+
+    def __init__(self, eng: Engine, jid: int, spec: SimSpec, precision):
+        self.eng, self.id, self.spec, self.precision = eng, jid, spec, precision
+        self.steps = 0
+        self.released = False
+
+    def advance(self, nsteps: int):
+        self.eng._check(self.eng.lib.oidt_job_advance(self.eng.ctx, self.id, nsteps))
+        self.steps += nsteps
+        return self
+
+    def run(self):
+        """Advance through every remaining source step."""
+        return self.advance(self.spec.nt - self.steps)
+
+    def sync(self, timeout_ms: int = -1):
+        self.eng._check(self.eng.lib.oidt_job_sync(self.eng.ctx, self.id, timeout_ms))
+        return self
+
+    def busy(self) -> bool:
+        done, busy = C.c_int32(), C.c_int32()
+        self.eng._check(self.eng.lib.oidt_job_query(self.eng.ctx, self.id, C.byref(done), C.byref(busy)))
+        return bool(busy.value)
+
+    def dft(self, port: int, comp) -> np.ndarray:
+        """complex128 DFT of one port component, reference layout."""
+        comps = DFT_COMPS[self.spec.mode]
+        ci = comps.index(comp) if isinstance(comp, str) else comp
+        plane = self.spec.shape[:2] if self.spec.mode == "yee3d" else (self.spec.shape[1],)
+        out = np.empty((self.spec.nf,) + tuple(plane), dtype=np.complex128)
+        self.eng._check(self.eng.lib.oidt_job_read_dft(self.eng.ctx, self.id, port, ci,
+                                                       out.ctypes.data, out.size * 2))
+        return out
+
+    def field(self, name: str) -> np.ndarray:
+        out = np.empty(self.spec.shape, dtype=self.precision)
+        self.eng._check(self.eng.lib.oidt_job_read_field(self.eng.ctx, self.id, FIELD_ID[name],
+                                                         out.ctypes.data, out.nbytes))
+        return out
+
+    def set_field(self, name: str, values: np.ndarray):
+        a = np.ascontiguousarray(values, dtype=self.precision)
+        if a.shape != tuple(self.spec.shape):
+            raise ValueError("field shape must be %s" % (self.spec.shape,))
+        self.eng._check(self.eng.lib.oidt_job_write_field(self.eng.ctx, self.id, FIELD_ID[name],
+                                                          a.ctypes.data, a.nbytes))
+
+    def psi(self, name: str, axis: int, side: int) -> np.ndarray:
+        out = np.empty(self.spec.psi_shape(axis), dtype=self.precision)
+        self.eng._check(self.eng.lib.oidt_job_read_psi(self.eng.ctx, self.id, FIELD_ID[name], axis, side,
+                                                       out.ctypes.data, out.nbytes))
+        return out
+
+    def fields(self) -> dict:
+        return {f: self.field(f) for f in FIELDS[self.spec.mode]}
+
+    def release(self):
+        if not self.released:
+            self.eng._check(self.eng.lib.oidt_job_release(self.eng.ctx, self.id))
+            self.released = True
+
+
+__all__ = ["Engine", "Job", "OidtError", "BudgetError", "load_library", "EXPORTS", "LIB_PATH", "PSI"]

@@ -1,0 +1,135 @@
+"""Engine job description (host side) and its C-ABI form.
+
+A :class:`SimSpec` carries every array and scalar one simulation needs, in
+the reference's layout and naming; :func:`to_desc` turns it into the
+``oidt_job_desc`` struct of ``include/oidt.h`` (host pointers that the
+library copies once at job creation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+MODE_ID = {"tm2": 0, "te2": 1, "yee3d": 2}
+FIELD_ID = {"EX": 0, "EY": 1, "EZ": 2, "HX": 3, "HY": 4, "HZ": 5}
+FIELDS = {"tm2": ("EZ", "HX", "HY"), "te2": ("EX", "EY", "HZ"), "yee3d": ("EX", "EY", "EZ", "HX", "HY", "HZ")}
+# DFT components per port, in ABI order (oidt_job_read_dft comp index)
+DFT_COMPS = {"tm2": ("ez", "hy"), "te2": ("ey", "hz"), "yee3d": ("ex", "ey", "hx", "hy")}
+# CPML psi arrays per solver: (field, slab axis)
+PSI = {"tm2": (("EZ", 0), ("EZ", 1), ("HX", 1), ("HY", 0)),
+       "te2": (("EX", 1), ("EY", 0), ("HZ", 0), ("HZ", 1)),
+       "yee3d": (("EX", 1), ("EX", 2), ("EY", 0), ("EY", 2), ("EZ", 0), ("EZ", 1),
+                 ("HX", 1), ("HX", 2), ("HY", 0), ("HY", 2), ("HZ", 0), ("HZ", 1))}
+
+
+@dataclass
+class SimSpec:
+    mode: str
+    precision: np.dtype
+    shape: tuple
+    num_cpml: int
+    lim_lo: tuple
+    lim_hi: tuple
+    cb: dict          # 'x'/'y'/'z' -> dt/eps grid of that E component
+    kdx: dict         # 'xe','xh','ye','yh'[,'ze','zh'] -> kappa*dx
+    be: np.ndarray
+    ce: np.ndarray
+    bh: np.ndarray
+    ch: np.ndarray
+    db: float
+    dx: float
+    src_field: int
+    src_lo: tuple
+    src_hi: tuple
+    j_src: np.ndarray
+    port_pos: tuple
+    win_lo: tuple
+    win_hi: tuple
+    freqs: np.ndarray
+    twiddles: tuple   # cosE, sinE, cosH, sinH, float64 [nf][nt]
+    nt: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def ncells(self) -> int:
+        return int(np.prod(self.shape))
+
+    @property
+    def nf(self) -> int:
+        return len(self.freqs)
+
+    def psi_shape(self, axis: int) -> tuple:
+        s = list(self.shape)
+        s[axis] = self.num_cpml
+        return tuple(s)
+
+
+class JobDesc(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32), ("precision", C.c_int32), ("arith", C.c_int32),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("num_cpml", C.c_int32),
+        ("ib", C.c_int32), ("jb", C.c_int32), ("kb", C.c_int32),
+        ("ie", C.c_int32), ("je", C.c_int32), ("ke", C.c_int32),
+        ("nt", C.c_int32), ("nf", C.c_int32),
+        ("cb", C.c_void_p * 3), ("kdx", C.c_void_p * 6),
+        ("be", C.c_void_p), ("ce", C.c_void_p), ("bh", C.c_void_p), ("ch", C.c_void_p),
+        ("db", C.c_double), ("dx", C.c_double),
+        ("src_field", C.c_int32), ("src_lo", C.c_int32 * 3), ("src_hi", C.c_int32 * 3),
+        ("j_src", C.c_void_p),
+        ("port_pos", C.c_int32 * 2), ("win_lo", C.c_int32 * 2), ("win_hi", C.c_int32 * 2),
+        ("cos_e", C.c_void_p), ("sin_e", C.c_void_p), ("cos_h", C.c_void_p), ("sin_h", C.c_void_p),
+        ("ring_steps", C.c_int32), ("reserved", C.c_int32 * 7),
+    ]
+
+
+def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0):
+    """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
+    ``keepalive`` must outlive the ``oidt_job_create`` call."""
+    prec = np.dtype(precision if precision is not None else spec.precision)
+    if prec not in (np.dtype(np.float32), np.dtype(np.float64)):
+        raise ValueError("precision must be float32 or float64")
+    keep = []
+
+    def arr(a, dt=prec):
+        a = np.ascontiguousarray(np.asarray(a, dtype=dt))
+        keep.append(a)
+        return a.ctypes.data
+
+    d = JobDesc()
+    d.mode = MODE_ID[spec.mode]
+    d.precision = 0 if prec == np.float32 else 1
+    d.arith = {"fast": 0, "exact": 1}[arith]
+    sh = tuple(spec.shape) + ((1,) if len(spec.shape) == 2 else ())
+    d.nx, d.ny, d.nz = sh
+    d.num_cpml = spec.num_cpml
+    lo = tuple(spec.lim_lo) + ((0,) if len(spec.shape) == 2 else ())
+    hi = tuple(spec.lim_hi) + ((1,) if len(spec.shape) == 2 else ())
+    d.ib, d.jb, d.kb = lo
+    d.ie, d.je, d.ke = hi
+    d.nt = spec.nt
+    d.nf = spec.nf
+    for slot, ax in enumerate("xyz"):
+        if ax in spec.cb:
+            d.cb[slot] = arr(spec.cb[ax])
+    for slot, key in enumerate(("xe", "ye", "ze", "xh", "yh", "zh")):
+        if key in spec.kdx:
+            d.kdx[slot] = arr(spec.kdx[key])
+    d.be, d.ce, d.bh, d.ch = arr(spec.be), arr(spec.ce), arr(spec.bh), arr(spec.ch)
+    d.db = float(spec.db)
+    d.dx = float(spec.dx)
+    d.src_field = spec.src_field
+    for a in range(3):
+        d.src_lo[a] = spec.src_lo[a] if a < len(spec.src_lo) else 0
+        d.src_hi[a] = spec.src_hi[a] if a < len(spec.src_hi) else 1
+    js = np.zeros(spec.nt, dtype=prec)
+    js[:len(spec.j_src)] = spec.j_src[:spec.nt]
+    d.j_src = arr(js)
+    d.port_pos[0], d.port_pos[1] = spec.port_pos
+    d.win_lo[0], d.win_lo[1] = spec.win_lo
+    d.win_hi[0], d.win_hi[1] = spec.win_hi
+    tw = [arr(t, np.float64) for t in spec.twiddles]
+    d.cos_e, d.sin_e, d.cos_h, d.sin_h = tw
+    d.ring_steps = ring_steps
+    return d, keep

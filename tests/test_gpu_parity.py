@@ -1,0 +1,174 @@
+"""Engine parity on a B200, through the C ABI (liboidt.so).
+
+* float64 with OIDT_ARITH_EXACT must equal, bit for bit, (a) the reference's
+  own device arrays recorded under Numba's CUDA simulator (golden fixtures)
+  and (b) the float64 oracle, on random initial fields that exercise every
+  CPML slab, the source and the port planes at once.
+* float32 with OIDT_ARITH_FAST (the production path) against the float64
+  oracle on identical inputs: field relative L2 <= 1e-5 and
+  |S_fp32 - S_oracle| <= 1e-4 (the stated precision targets).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import fdtd_ref as R
+from tests import golden_io as G
+from tests.helpers import oracle_from_spec, psi_key, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-5
+S_TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from oidt_b200.engine import Engine
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+def _fixture_cases():
+    out = []
+    for case in ["tm2_smooth", "tm2_rough2", "te2_smooth", "te2_rough2", "yee3d_smooth", "yee3d_rough2_tm"]:
+        if os.path.exists(os.path.join(G.GOLDEN, case + ".npz")):
+            out.append(case)
+    return out
+
+
+@pytest.mark.parametrize("case", _fixture_cases())
+def test_exact_f64_equals_reference_device_arrays(eng, case):
+    """Engine float64 EXACT == the reference's recorded device arrays."""
+    from oidt_b200.refsetup import build_spec
+    z = G.load(case)
+    usr = G.usr_of(z)
+    mode = case.split("_")[0]
+    for (line, d, kind) in G.sims_of(z):
+        tag = "%d%s%s" % (line, d, kind)
+        spec = build_spec(usr, mode, line, d, kind, profiles=G.profiles_of(z))
+        job = eng.submit(spec, arith="exact", precision=np.float64, ring_steps=5)
+        job.run().sync(60000)
+        for f, arr in job.fields().items():
+            np.testing.assert_array_equal(arr, z["%s/dev_%s" % (tag, f)], err_msg="%s %s" % (tag, f))
+        from oidt_b200.spec import PSI
+        for name, axis in PSI[mode]:
+            for side in (0, 1):
+                np.testing.assert_array_equal(job.psi(name, axis, side), z["%s/dev_%s" % (tag, psi_key(name, axis, side))])
+        comps = {"tm2": ("EZ", "HY"), "te2": ("EY", "HZ"), "yee3d": ("EX", "EY", "HX", "HY")}[mode]
+        for port in (0, 1):
+            for ci, cn in enumerate(comps):
+                ref = z["%s/dev_%s%dr" % (tag, cn, port + 1)] + 1j * z["%s/dev_%s%di" % (tag, cn, port + 1)]
+                np.testing.assert_array_equal(job.dft(port, ci), ref, err_msg="%s port %d %s" % (tag, port, cn))
+        job.release()
+
+
+def _random_cases():
+    from oidt_b200 import workloads as W
+    return {
+        "tm2": lambda: W.slab2d(nx=70, ny=61, P=5, core_cells=9, src_x=12, ports=(20, 50), steps=40, nf=5,
+                                rough=True, sigma_nm=30, lc_nm=60, seed=3),
+        "yee3d_te": lambda: W.strip3d(nx=22, ny=19, nz=37, P=4, src_gap=2, port_gap=3, steps=40, nf=4,
+                                      core_x_nm=120, core_y_nm=160, sigma_nm=25, lc_nm=60, seed=5),
+        "yee3d_tm": lambda: W.strip3d(nx=21, ny=24, nz=33, P=3, src_gap=2, port_gap=3, steps=40, nf=3,
+                                      core_x_nm=140, core_y_nm=180, source="TM", seed=6),
+    }
+
+
+def _te2_spec():
+    """A TE2 job: reuse the slab geometry with the TE solver arrays."""
+    from oidt_b200 import workloads as W
+    s = W.slab2d(nx=66, ny=57, P=4, core_cells=9, src_x=12, ports=(20, 46), steps=40, nf=4)
+    s.mode = "te2"
+    from oidt_b200.refsetup import staggered_eps
+    eps_cell = s.meta["dt"] / s.cb["z"]
+    ex, ey = staggered_eps(eps_cell, np.float64, (0, 1))
+    s.cb = {"x": s.meta["dt"] / ex, "y": s.meta["dt"] / ey}
+    by = s.src_lo[1] - 1
+    s.src_field = 5  # HZ
+    s.src_lo = (12, by + 2, 0)
+    s.src_hi = (13, by + 9 - 2, 1)
+    return s
+
+
+@pytest.mark.parametrize("name", ["tm2", "te2", "yee3d_te", "yee3d_tm"])
+@pytest.mark.parametrize("ring", [1, 7, 32])
+def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
+    spec = _te2_spec() if name == "te2" else _random_cases()[name]()
+    rng = np.random.default_rng(abs(hash(name)) % 1000 + ring)
+    s = oracle_from_spec(spec)
+    job = eng.submit(spec, arith="exact", precision=np.float64, ring_steps=ring)
+    for f in R.field_names(spec.mode):
+        v = rng.standard_normal(spec.shape) * 1e-2
+        getattr(s, f)[...] = v
+        job.set_field(f, v)
+    nsteps = 23
+    job.advance(10).advance(nsteps - 10).sync(60000)
+    R.run(s, nsteps)
+    for f, arr in job.fields().items():
+        np.testing.assert_array_equal(arr, getattr(s, f), err_msg=f)
+    from oidt_b200.spec import PSI
+    for fname, axis in PSI[spec.mode]:
+        for side in (0, 1):
+            np.testing.assert_array_equal(job.psi(fname, axis, side), getattr(s, psi_key(fname, axis, side)))
+    ncomp = 4 if spec.mode == "yee3d" else 2
+    for port in (0, 1):
+        for c in range(ncomp):
+            np.testing.assert_array_equal(job.dft(port, c), R.dft_complex(s, port, c), err_msg="port %d comp %d" % (port, c))
+    job.release()
+
+
+def _s_forward(spec, dfts_inc, dfts_ref):
+    from oidt_b200.sparams import forward_s
+    return forward_s(spec, dfts_inc, dfts_ref)
+
+
+def test_fp32_slab2d_full_run_within_targets(eng):
+    """The 400 x 200, 2000-step 2D case: float32 engine vs float64 oracle."""
+    from oidt_b200 import workloads as W
+    from oidt_b200.sparams import forward_s
+    from tests.helpers import dft_dict_oracle
+    spec = W.slab2d()
+    job = eng.submit(spec, arith="fast", precision=np.float32)
+    job.run().sync(120000)
+    s = oracle_from_spec(spec)
+    R.run(s, spec.nt)
+    for f in ("EZ", "HX", "HY"):
+        err = rel_l2(job.field(f), getattr(s, f))
+        assert err <= FIELD_TOL, (f, err)
+    d_eng = {(p, c): job.dft(p, c) for p in (0, 1) for c in (0, 1)}
+    d_ora = dft_dict_oracle(s)
+    for k in d_eng:
+        assert rel_l2(d_eng[k], d_ora[k]) <= S_TOL, k
+    S_e = forward_s(spec, d_eng, d_eng)
+    S_o = forward_s(spec, d_ora, d_ora)
+    assert np.max(np.abs(S_e["S21"] - S_o["S21"])) <= S_TOL
+    job.release()
+
+
+def test_fp32_strip3d_within_targets(eng):
+    """A reduced 3D rough strip (64 x 56 x 120, 700 steps) in float32 vs the
+    float64 oracle on identical inputs."""
+    from oidt_b200 import workloads as W
+    from oidt_b200.sparams import forward_s
+    from tests.helpers import dft_dict_oracle
+    kw = dict(nx=64, ny=56, nz=120, P=8, steps=700, nf=9, src_gap=4, port_gap=10)
+    spec_r = W.strip3d(**kw)
+    spec_i = W.strip3d(rough=False, **kw)
+    out = {}
+    for tag, spec in (("i", spec_i), ("r", spec_r)):
+        job = eng.submit(spec, arith="fast", precision=np.float32)
+        job.run().sync(120000)
+        s = oracle_from_spec(spec)
+        R.run(s, spec.nt)
+        for f in R.field_names("yee3d"):
+            err = rel_l2(job.field(f), getattr(s, f))
+            assert err <= FIELD_TOL, (tag, f, err)
+        out[tag] = ({(p, c): job.dft(p, c) for p in (0, 1) for c in range(4)}, dft_dict_oracle(s))
+        job.release()
+    S_e = forward_s(spec_r, out["i"][0], out["r"][0])
+    S_o = forward_s(spec_r, out["i"][1], out["r"][1])
+    for k in ("S11", "S21"):
+        assert np.max(np.abs(S_e[k] - S_o[k])) <= S_TOL, k
