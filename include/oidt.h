@@ -157,6 +157,23 @@ int32_t oidt_job_read_psi(oidt_ctx *ctx, uint64_t job, int32_t field, int32_t ax
 
 int32_t oidt_job_release(oidt_ctx *ctx, uint64_t job);
 
+/* Return the job to step 0 (zero fields, psi, capture ring, DFT
+ * accumulators) keeping its coefficients resident: the next simulation on the
+ * same structure without another host-to-device copy.  The reference has no
+ * counterpart (it starts a new process per simulation, fdtd_main.py:51-53). */
+int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job);
+
+/* The context's compute stream (a cudaStream_t), so callers can order their
+ * own work or record CUDA events around oidt_job_advance. */
+int32_t oidt_ctx_stream(oidt_ctx *ctx, void **stream);
+
+/* Run nsteps steps without graph replay, bracketing every launch with CUDA
+ * events on the compute stream; ms_out[0..2] receive the average duration of
+ * the E-half, H-half and DFT-fold launches.  Replaces the reference's
+ * wall-clock MCells/s print (fdtd_main.py:306-341) with per-kernel device
+ * times. */
+int32_t oidt_job_profile(oidt_ctx *ctx, uint64_t job, int32_t nsteps, float *ms_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,10 +9,10 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = [os.path.join(HERE, "csrc", "engine.cu")]
+SRC = [os.path.join(HERE, "csrc", "engine.cu")]  # includes kernels.cuh and sweep3d.cuh
 DEPS = SRC + [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))] + \
     [os.path.join(ROOT, "include", "oidt.h")]
-LIB = os.path.join(HERE, "liboidt.so")
+LIB = os.environ.get("OIDT_LIB_OUT", os.path.join(HERE, "liboidt.so"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC,-O2", "-shared", "--expt-relaxed-constexpr"]

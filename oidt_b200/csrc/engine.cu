@@ -1,17 +1,22 @@
 // engine.cu -- liboidt.so: job management, launches and the C ABI (include/oidt.h).
 //
 // Device layout of one job (one cudaMallocAsync block, 256-byte aligned
-// sub-buffers): fields and coefficient grids in the reference layout
-// ([nx][ny] or [nx][ny][nz], C order), 1-D kappa*dx arrays and their
+// sub-buffers): fields and dt/eps grids in the reference layout ([nx][ny] or
+// [nx][ny][nz], C order; 3D rows along z padded to a multiple of 4 cells so
+// TMA row strides are 16-byte multiples), 1-D kappa*dx arrays and their
 // reciprocals, CPML psi slabs in the reference's PSI_<F>_<A><LO|HI> shapes,
 // the source waveform, float64 twiddle tables [nf][nt], the capture ring
-// [K][port][slot][plane] and the float64 complex DFT accumulators
-// [port][comp][nf][plane].
+// [K][port][slot][plane], float64 complex DFT accumulators
+// [port][comp][nf][plane], and for 3D a second field buffer and a second
+// E-psi buffer (the plane sweep writes the other buffer each step).
 //
-// A time step is two launches (E half, H half; kernels.cuh).  Every K steps a
-// fold kernel turns the K captured port planes into float64 DFT updates and a
-// one-thread kernel advances the job's step counter, so a K-step block is a
-// fixed launch sequence that is captured once into a CUDA graph and replayed.
+// A 3D time step is one launch of the plane sweep (sweep3d.cuh) over the job's
+// work items; 2D steps (and the 3D per-cell variant) are two launches (E
+// half, H half; kernels.cuh).  Every K steps a fold kernel turns the captured
+// port planes into float64 DFT updates and a one-thread kernel advances the
+// step counter, so a K-step block is a fixed launch sequence that is captured
+// once into a CUDA graph and replayed.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -19,6 +24,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -28,18 +34,21 @@
 
 #include "../../include/oidt.h"
 #include "kernels.cuh"
+#include "sweep3d.cuh"
 
 using namespace oidt;
 
 namespace {
 
 constexpr int kDefaultRing = 32;
-constexpr int kFoldF = 8;        // frequencies per fold thread
+constexpr int kFoldF = 8;  // frequencies per fold thread
 constexpr int kBlock3Z = 32, kBlock3Y = 4;
 constexpr int kBlock2 = 128;
+constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;
+constexpr int kVariantSweep = 0, kVariantCell = 1;
 
 // ---------------------------------------------------------------------------
-// Kernels: single-job and multi-job launches of the per-cell updates.
+// Per-cell launches (2D, and the 3D per-cell variant): in place.
 // ---------------------------------------------------------------------------
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128) k_y3_e(Params<T> p, int s) {
@@ -72,9 +81,9 @@ __global__ void __launch_bounds__(128) k_2d_h(Params<T> p, int s) {
     te2_h_cell<T, EXACT>(p, i, j, p.state[0] + s, s);
 }
 
-// Multi-job launch: block b works on tile tiles[b] = {job, i, j0, k0} of the
-// job whose parameters live at params[job] (device memory).  3D tiles are
-// 32 (k) x 4 (j) cells of one x-plane, 2D tiles 128 (j) cells of one x-line.
+// Multi-job per-cell launch: block b works on tile tiles[b] = {job, i, j0, k0}
+// of the job whose in-place parameters are params[job] (device memory).  3D
+// tiles are 32 (k) x 4 (j) cells of one x-plane, 2D tiles 128 (j) cells.
 struct Tile {
   int job, i, j0, k0;
 };
@@ -114,7 +123,7 @@ __global__ void __launch_bounds__(128) k_batch(const Params<T> *__restrict__ par
 // in float64, s = 0..count-1 in order (the reference's running sum, one step
 // at a time: fdtd_funcs.py simul_fft_efield/hfield).  x_s is the colocated
 // port-plane sample computed from the captured raw planes:
-//   TM2 E: Ez[ic,j]                 H: (Hy[ic,j] + Hy[ic+1,j]) / 2
+//   TM2 E: Ez[ic,j]                   H: (Hy[ic,j] + Hy[ic+1,j]) / 2
 //   TE2 E: (Ey[ic,j] + Ey[ic,j+1])/2  H: 4-point Hz average
 //   3D  Ex: (Ex[i,j] + Ex[i+1,j])/2, Ey: (Ey[i,j] + Ey[i,j+1])/2,
 //       Hx, Hy: 4-point averages over (j or i) x (kc, kc+1).
@@ -219,6 +228,7 @@ struct Layout {
 
 int ncomp_of(int mode) { return mode == OIDT_MODE_YEE3D ? 4 : 2; }
 int nslot_of(int mode) { return mode == OIDT_MODE_YEE3D ? 6 : 3; }
+bool is_e(int f) { return f <= EZ; }
 
 // (field, slab axis) pairs with CPML psi arrays per solver, in the reference's
 // PSI_<F>_<A> naming.
@@ -248,12 +258,46 @@ long long psi_elems(int mode, int axis, int nx, int ny, int nz, int P) {
 
 struct JobPlan {
   size_t total;
-  size_t off_f[6], off_cb[3], off_kd[6], off_rkd[6], off_be, off_ce, off_bh, off_ch;
-  size_t off_psi[6][3][2];
-  size_t off_jsrc, off_tw[4], off_ring, off_acc, off_state, off_params;
+  size_t off_f[2][6], off_cb[3], off_kd[6], off_rkd[6], off_be, off_ce, off_bh, off_ch;
+  size_t off_psi[2][6][3][2];
+  size_t off_jsrc, off_tw[4], off_ring, off_acc, off_state, off_params, off_tmaps, off_items, off_zero;
   long long N, plane;
-  int K, esz;
+  int K, esz, nzp, nbuf, variant, L, nitems;
 };
+
+// Work items of one 3D job: tiles of TY x TZ cells in (y, z), chunks of L
+// planes in x over the updated planes [ib, ie).
+std::vector<SweepItem> sweep_items(const oidt_job_desc *d, int L, int job) {
+  std::vector<SweepItem> v;
+  for (int x0 = d->ib; x0 < d->ie; x0 += L)
+    for (int y0 = 0; y0 < d->ny; y0 += TY)
+      for (int z0 = 0; z0 < d->nz; z0 += TZ) v.push_back({job, y0, z0, x0, std::min(x0 + L, d->ie)});
+  return v;
+}
+
+// March depth: the chunk length that best fills whole waves of resident CTAs
+// (item cost ~ L + 2 planes, the extra planes being the E and H halos along
+// x).  OIDT_SWEEP_L overrides.  `slots` = SMs x resident CTAs per SM.
+int choose_chunk(const oidt_job_desc *d, int slots) {
+  if (const char *e = getenv("OIDT_SWEEP_L")) {
+    int v = atoi(e);
+    if (v > 0) return v;
+  }
+  const int planes = d->ie - d->ib;
+  const long long tiles = (long long)((d->ny + TY - 1) / TY) * ((d->nz + TZ - 1) / TZ);
+  double best = 1e300;
+  int bestL = planes;
+  for (int L = 4; L <= planes; ++L) {
+    const long long chunks = (planes + L - 1) / L;
+    const long long items = tiles * chunks;
+    const long long waves = (items + slots - 1) / slots;
+    const double cost = (double)waves * (L + 2);  // critical path in plane-iterations
+    if (cost < best - 1e-9) { best = cost; bestL = L; }
+  }
+  return bestL;
+}
+
+int g_sweep_slots = 0;  // SMs x resident sweep CTAs (set at context creation)
 
 int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   auto bad = [&](const char *m) { if (why) *why = m; return OIDT_ERR_INVALID; };
@@ -279,11 +323,9 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
     if (!d->cb[c]) return bad("missing cb array");
   for (int a = 0; a < 6; ++a)
     if (!d->kdx[a] && (is3 || (a != 2 && a != 5))) return bad("missing kappa*dx array");
-  const int along = is3 ? 2 : 0;  // port planes: z (3D) or x (2D)
   const int nalong = is3 ? d->nz : d->nx;
   for (int q = 0; q < 2; ++q)
     if (d->port_pos[q] < 0 || d->port_pos[q] + 1 >= nalong) return bad("port plane out of range");
-  (void)along;
   if (d->win_lo[1] < 0 || d->win_hi[1] > d->ny - 1 || d->win_lo[1] >= d->win_hi[1]) return bad("bad DFT window (j)");
   if (is3 && (d->win_lo[0] < 0 || d->win_hi[0] > d->nx - 1 || d->win_lo[0] >= d->win_hi[0]))
     return bad("bad DFT window (i)");
@@ -298,14 +340,19 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
         return bad("source box must lie inside the updated interior");
     }
   }
+  const int variant = is3 ? (d->reserved[0] == kVariantCell ? kVariantCell : kVariantSweep) : kVariantCell;
   const int esz = d->precision == OIDT_F32 ? 4 : 8;
-  const long long N = (long long)d->nx * d->ny * d->nz;
+  const int nzp = is3 ? (int)align_up(d->nz, 4) : 1;
+  const long long N = (long long)d->nx * d->ny * nzp;
   const long long plane = is3 ? (long long)d->nx * d->ny : d->ny;
-  const int K = d->ring_steps > 0 ? d->ring_steps : kDefaultRing;
+  int K = d->ring_steps > 0 ? d->ring_steps : kDefaultRing;
   if (K > 4096) return bad("ring_steps too large");
+  if (variant == kVariantSweep && (K & 1)) ++K;  // graphs of the sweep end on the parity they start
+  const int nbuf = variant == kVariantSweep ? 2 : 1;
   Layout L;
   memset(pl, 0, sizeof(*pl));
-  for (int f : fields_of(d->mode)) pl->off_f[f] = L.take(N * esz);
+  for (int b = 0; b < nbuf; ++b)
+    for (int f : fields_of(d->mode)) pl->off_f[b][f] = L.take(N * esz);
   for (int c : cb_of(d->mode)) pl->off_cb[c] = L.take(N * esz);
   const int dims[3] = {d->nx, d->ny, d->nz};
   for (int a = 0; a < 6; ++a) {
@@ -318,19 +365,30 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->off_bh = L.take(P * esz);
   pl->off_ch = L.take(P * esz);
   for (auto fa : psi_pairs(d->mode))
-    for (int sd = 0; sd < 2; ++sd)
-      pl->off_psi[fa.first][fa.second][sd] = L.take(psi_elems(d->mode, fa.second, d->nx, d->ny, d->nz, P) * esz);
+    for (int b = 0; b < (is_e(fa.first) ? nbuf : 1); ++b)
+      for (int sd = 0; sd < 2; ++sd)
+        pl->off_psi[b][fa.first][fa.second][sd] = L.take(psi_elems(d->mode, fa.second, d->nx, d->ny, d->nz, P) * esz);
   pl->off_jsrc = L.take((size_t)d->nt * esz);
   for (int t = 0; t < 4; ++t) pl->off_tw[t] = L.take((size_t)d->nf * d->nt * 8);
   pl->off_ring = L.take((size_t)K * 2 * nslot_of(d->mode) * plane * esz);
   pl->off_acc = L.take((size_t)2 * ncomp_of(d->mode) * d->nf * plane * 16);
   pl->off_state = L.take(64);
-  pl->off_params = L.take(std::max(sizeof(Params<float>), sizeof(Params<double>)));
+  pl->off_zero = pl->off_state + 32;  // a device int 0 (parity base of a single job)
+  pl->off_params = L.take(4 * std::max(sizeof(Params<float>), sizeof(Params<double>)));
+  if (variant == kVariantSweep) {
+    pl->off_tmaps = L.take(15 * 128);
+    pl->L = choose_chunk(d, g_sweep_slots > 0 ? g_sweep_slots : 148 * 3);
+    pl->nitems = (int)sweep_items(d, pl->L, 0).size();
+    pl->off_items = L.take((size_t)pl->nitems * sizeof(SweepItem));
+  }
   pl->total = L.off;
   pl->N = N;
   pl->plane = plane;
   pl->K = K;
   pl->esz = esz;
+  pl->nzp = nzp;
+  pl->nbuf = nbuf;
+  pl->variant = variant;
   return OIDT_OK;
 }
 
@@ -339,22 +397,32 @@ struct Job {
   oidt_job_desc d{};
   JobPlan pl{};
   unsigned char *mem = nullptr;
-  Params<float> pf{};
-  Params<double> pd{};
+  // pv[b]: view with buffer b old (sweep reads b, writes b^1); pc[b]: in place on b
+  Params<float> pvf[2]{}, pcf[2]{};
+  Params<double> pvd[2]{}, pcd[2]{};
   FoldParams<float> ff{};
   FoldParams<double> fd{};
-  cudaGraphExec_t graph = nullptr;
-  cudaEvent_t ready = nullptr;  // uploads finished
-  cudaEvent_t done = nullptr;   // last enqueued work finished
+  int parity = 0;                                 // buffer holding the current state
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // K-step block starting at parity 0 / 1
+  long long graph_launches = 0;                   // kernels per graph replay
+  cudaEvent_t ready = nullptr;                    // uploads finished
+  cudaEvent_t done = nullptr;                     // last enqueued work finished
   long long steps_enqueued = 0;
   bool busy = false;
 };
 
 struct BatchPlan {  // cached multi-job composition
   std::vector<uint64_t> ids;
+  std::vector<int> pars;
+  unsigned char *mem = nullptr;
   Tile *tiles = nullptr;
   int ntiles = 0;
+  SweepItem *items = nullptr;
+  int nitems = 0;
+  void *pcell = nullptr, *pview = nullptr;
+  int *par0 = nullptr;
   cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;
   int K = 0;
 };
 
@@ -391,60 +459,133 @@ int fail(oidt_ctx *ctx, int code, const char *fmt, ...) {
     if (e_ != cudaSuccess) return fail(ctx, OIDT_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
-template <typename T> Params<T> &params_of(Job *j);
-template <> Params<float> &params_of<float>(Job *j) { return j->pf; }
-template <> Params<double> &params_of<double>(Job *j) { return j->pd; }
+template <typename T> Params<T> *views(Job *j);
+template <> Params<float> *views<float>(Job *j) { return j->pvf; }
+template <> Params<double> *views<double>(Job *j) { return j->pvd; }
+template <typename T> Params<T> *cells(Job *j);
+template <> Params<float> *cells<float>(Job *j) { return j->pcf; }
+template <> Params<double> *cells<double>(Job *j) { return j->pcd; }
 template <typename T> FoldParams<T> &fold_of(Job *j);
 template <> FoldParams<float> &fold_of<float>(Job *j) { return j->ff; }
 template <> FoldParams<double> &fold_of<double>(Job *j) { return j->fd; }
+
+// ---- tensor maps (TMA descriptors) ----------------------------------------
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void *p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+// 3D map over a pitched [nx][ny][nzp] array; box [1][TY+2][TZ+8] (z fastest).
+bool encode_map(CUtensorMap *m, void *base, int esz, int nzp, int ny, int nx) {
+  EncodeTiled enc = encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nzp, (cuuint64_t)ny, (cuuint64_t)nx};
+  const cuuint64_t strides[2] = {(cuuint64_t)nzp * esz, (cuuint64_t)ny * nzp * esz};
+  const cuuint32_t box[3] = {(cuuint32_t)(TZ + 8), (cuuint32_t)(TY + 2), 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return enc(m, esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 template <typename T> void fill_params(Job *J) {
   const oidt_job_desc &d = J->d;
   const JobPlan &pl = J->pl;
   unsigned char *m = J->mem;
-  Params<T> &p = params_of<T>(J);
-  memset(&p, 0, sizeof p);
-  p.mode = d.mode;
-  p.nx = d.nx; p.ny = d.ny; p.nz = d.nz;
-  p.P = d.num_cpml;
-  p.ib = d.ib; p.jb = d.jb; p.kb = d.kb; p.ie = d.ie; p.je = d.je; p.ke = d.ke;
-  for (int f : fields_of(d.mode)) p.f[f] = reinterpret_cast<T *>(m + pl.off_f[f]);
-  for (int c : cb_of(d.mode)) p.cb[c] = reinterpret_cast<const T *>(m + pl.off_cb[c]);
-  for (int a = 0; a < 6; ++a) {
-    if (d.mode != OIDT_MODE_YEE3D && (a == 2 || a == 5)) continue;
-    p.kd[a] = reinterpret_cast<const T *>(m + pl.off_kd[a]);
-    p.rkd[a] = reinterpret_cast<const T *>(m + pl.off_rkd[a]);
+  for (int b = 0; b < 2; ++b) {
+    Params<T> &p = cells<T>(J)[b];
+    memset(&p, 0, sizeof p);
+    p.mode = d.mode;
+    p.nx = d.nx; p.ny = d.ny; p.nz = d.nz; p.nzp = pl.nzp;
+    p.P = d.num_cpml;
+    p.ib = d.ib; p.jb = d.jb; p.kb = d.kb; p.ie = d.ie; p.je = d.je; p.ke = d.ke;
+    const int bb = b < pl.nbuf ? b : 0;
+    for (int f : fields_of(d.mode)) {
+      p.f[f] = reinterpret_cast<T *>(m + pl.off_f[bb][f]);
+      p.fn[f] = reinterpret_cast<T *>(m + pl.off_f[pl.nbuf == 2 ? bb ^ 1 : 0][f]);
+    }
+    for (int c : cb_of(d.mode)) p.cb[c] = reinterpret_cast<const T *>(m + pl.off_cb[c]);
+    for (int a = 0; a < 6; ++a) {
+      if (d.mode != OIDT_MODE_YEE3D && (a == 2 || a == 5)) continue;
+      p.kd[a] = reinterpret_cast<const T *>(m + pl.off_kd[a]);
+      p.rkd[a] = reinterpret_cast<const T *>(m + pl.off_rkd[a]);
+    }
+    p.be = reinterpret_cast<const T *>(m + pl.off_be);
+    p.ce = reinterpret_cast<const T *>(m + pl.off_ce);
+    p.bh = reinterpret_cast<const T *>(m + pl.off_bh);
+    p.ch = reinterpret_cast<const T *>(m + pl.off_ch);
+    p.db = (T)d.db;
+    p.dx = (T)d.dx;
+    p.rdx = (T)(1.0 / (double)p.dx);
+    for (auto fa : psi_pairs(d.mode))
+      for (int sd = 0; sd < 2; ++sd) {
+        const bool two = is_e(fa.first) && pl.nbuf == 2;
+        p.psi[fa.first][fa.second][sd] = reinterpret_cast<T *>(m + pl.off_psi[two ? bb : 0][fa.first][fa.second][sd]);
+        p.psin[fa.first][fa.second][sd] = p.psi[fa.first][fa.second][sd];  // in place
+      }
+    p.src_field = d.src_field;
+    for (int a = 0; a < 3; ++a) { p.slo[a] = d.src_lo[a]; p.shi[a] = d.src_hi[a]; }
+    if (d.mode != OIDT_MODE_YEE3D) { p.slo[2] = 0; p.shi[2] = 1; }
+    p.jsrc = reinterpret_cast<const T *>(m + pl.off_jsrc);
+    p.ring = reinterpret_cast<T *>(m + pl.off_ring);
+    p.ring_K = pl.K;
+    p.nslot = nslot_of(d.mode);
+    p.plane = pl.plane;
+    p.port_pos[0] = d.port_pos[0];
+    p.port_pos[1] = d.port_pos[1];
+    p.state = reinterpret_cast<int *>(m + pl.off_state);
+    // sweep view: read buffer b, write the other; E psi likewise
+    Params<T> &v = views<T>(J)[b];
+    v = p;
+    if (pl.nbuf == 2) {
+      for (auto fa : psi_pairs(d.mode))
+        if (is_e(fa.first))
+          for (int sd = 0; sd < 2; ++sd)
+            v.psin[fa.first][fa.second][sd] = reinterpret_cast<T *>(m + pl.off_psi[bb ^ 1][fa.first][fa.second][sd]);
+      v.tmap_f = m + pl.off_tmaps + (size_t)bb * 6 * 128;
+      v.tmap_cb = m + pl.off_tmaps + 12 * 128;
+    }
   }
-  p.be = reinterpret_cast<const T *>(m + pl.off_be);
-  p.ce = reinterpret_cast<const T *>(m + pl.off_ce);
-  p.bh = reinterpret_cast<const T *>(m + pl.off_bh);
-  p.ch = reinterpret_cast<const T *>(m + pl.off_ch);
-  p.db = (T)d.db;
-  p.dx = (T)d.dx;
-  p.rdx = (T)(1.0 / (double)p.dx);
-  for (auto fa : psi_pairs(d.mode))
-    for (int sd = 0; sd < 2; ++sd) p.psi[fa.first][fa.second][sd] = reinterpret_cast<T *>(m + pl.off_psi[fa.first][fa.second][sd]);
-  p.src_field = d.src_field;
-  for (int a = 0; a < 3; ++a) { p.slo[a] = d.src_lo[a]; p.shi[a] = d.src_hi[a]; }
-  if (d.mode != OIDT_MODE_YEE3D) { p.slo[2] = 0; p.shi[2] = 1; }
-  p.jsrc = reinterpret_cast<const T *>(m + pl.off_jsrc);
-  p.ring = reinterpret_cast<T *>(m + pl.off_ring);
-  p.ring_K = pl.K;
-  p.nslot = nslot_of(d.mode);
-  p.plane = pl.plane;
-  p.port_pos[0] = d.port_pos[0];
-  p.port_pos[1] = d.port_pos[1];
-  p.state = reinterpret_cast<int *>(m + pl.off_state);
-
   FoldParams<T> &fp = fold_of<T>(J);
   memset(&fp, 0, sizeof fp);
   fp.mode = d.mode; fp.nx = d.nx; fp.ny = d.ny; fp.nf = d.nf; fp.nt = d.nt;
   fp.nslot = nslot_of(d.mode); fp.ncomp = ncomp_of(d.mode); fp.plane = pl.plane;
-  fp.ring = p.ring;
+  fp.ring = reinterpret_cast<T *>(m + pl.off_ring);
   fp.acc = reinterpret_cast<double2 *>(m + pl.off_acc);
   for (int t = 0; t < 4; ++t) fp.tw[t] = reinterpret_cast<const double *>(m + pl.off_tw[t]);
   fp.wlo0 = d.win_lo[0]; fp.whi0 = d.win_hi[0]; fp.wlo1 = d.win_lo[1]; fp.whi1 = d.win_hi[1];
-  fp.state = p.state;
+  fp.state = reinterpret_cast<int *>(m + pl.off_state);
+}
+
+// Host array (dense reference layout) <-> pitched device grid.
+int copy_grid_h2d(oidt_ctx *ctx, Job *J, void *dst, const void *src, cudaStream_t st) {
+  const JobPlan &pl = J->pl;
+  const size_t row = (size_t)J->d.nz * pl.esz, pitch = (size_t)pl.nzp * pl.esz, rows = (size_t)J->d.nx * J->d.ny;
+  if (row == pitch)
+    CU(ctx, cudaMemcpyAsync(dst, src, row * rows, cudaMemcpyHostToDevice, st));
+  else
+    CU(ctx, cudaMemcpy2DAsync(dst, pitch, src, row, row, rows, cudaMemcpyHostToDevice, st));
+  return OIDT_OK;
+}
+int copy_grid_d2h(oidt_ctx *ctx, Job *J, void *dst, const void *src) {
+  const JobPlan &pl = J->pl;
+  const size_t row = (size_t)J->d.nz * pl.esz, pitch = (size_t)pl.nzp * pl.esz, rows = (size_t)J->d.nx * J->d.ny;
+  if (row == pitch)
+    CU(ctx, cudaMemcpy(dst, src, row * rows, cudaMemcpyDeviceToHost));
+  else
+    CU(ctx, cudaMemcpy2D(dst, row, src, pitch, row, rows, cudaMemcpyDeviceToHost));
+  return OIDT_OK;
 }
 
 template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src) {
@@ -453,8 +594,10 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
   unsigned char *m = J->mem;
   cudaStream_t st = ctx->upload;
   CU(ctx, cudaMemsetAsync(m, 0, pl.total, st));
-  const size_t N = pl.N * sizeof(T);
-  for (int c : cb_of(d.mode)) CU(ctx, cudaMemcpyAsync(m + pl.off_cb[c], d.cb[c], N, cudaMemcpyHostToDevice, st));
+  for (int c : cb_of(d.mode)) {
+    int rc = copy_grid_h2d(ctx, J, m + pl.off_cb[c], d.cb[c], st);
+    if (rc) return rc;
+  }
   const int dims[3] = {d.nx, d.ny, d.nz};
   std::vector<T> rk;
   for (int a = 0; a < 6; ++a) {
@@ -477,15 +620,46 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
   for (int t = 0; t < 4; ++t)
     CU(ctx, cudaMemcpyAsync(m + pl.off_tw[t], tw[t], (size_t)d.nf * d.nt * 8, cudaMemcpyHostToDevice, st));
   fill_params<T>(J);
-  CU(ctx, cudaMemcpyAsync(m + pl.off_params, &params_of<T>(J), sizeof(Params<T>), cudaMemcpyHostToDevice, st));
+  CU(ctx, cudaMemcpyAsync(m + pl.off_params, views<T>(J), 2 * sizeof(Params<T>), cudaMemcpyHostToDevice, st));
+  if (pl.variant == kVariantSweep) {
+    std::vector<CUtensorMap> maps(15);
+    for (int b = 0; b < 2; ++b)
+      for (int f = 0; f < 6; ++f)
+        if (!encode_map(&maps[b * 6 + f], m + pl.off_f[b][f], pl.esz, pl.nzp, d.ny, d.nx))
+          return fail(ctx, OIDT_ERR_CUDA, "cuTensorMapEncodeTiled failed (field map)");
+    for (int c = 0; c < 3; ++c)
+      if (!encode_map(&maps[12 + c], m + pl.off_cb[c], pl.esz, pl.nzp, d.ny, d.nx))
+        return fail(ctx, OIDT_ERR_CUDA, "cuTensorMapEncodeTiled failed (cb map)");
+    CU(ctx, cudaMemcpyAsync(m + pl.off_tmaps, maps.data(), 15 * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
+    std::vector<SweepItem> it = sweep_items(&d, pl.L, 0);
+    CU(ctx, cudaMemcpyAsync(m + pl.off_items, it.data(), it.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, st));
+    CU(ctx, cudaStreamSynchronize(st));  // maps and items are host temporaries
+  }
   CU(ctx, cudaEventRecord(J->ready, st));
   // Host buffers are borrowed only for this call.
   CU(ctx, cudaStreamSynchronize(st));
   return OIDT_OK;
 }
 
-template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s, cudaStream_t st) {
-  Params<T> &p = params_of<T>(J);
+template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, TY, TZ, ST>(); }
+
+template <typename T, bool EXACT>
+void launch_sweep(const Params<T> *dparams, const int *dpar0, const SweepItem *items, int nitems, int par, int s,
+                  cudaStream_t st) {
+  k_sweep3d<T, EXACT, TY, TZ, ST><<<nitems, TY * TZ, sweep_smem<T>(), st>>>(dparams, dpar0, items, par, s);
+}
+
+// One time step of one job (s = step offset inside the K block, par = the
+// buffer holding the state at this step).
+template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s, int par, cudaStream_t st) {
+  if (J->pl.variant == kVariantSweep) {
+    const Params<T> *dp = reinterpret_cast<const Params<T> *>(J->mem + J->pl.off_params);
+    launch_sweep<T, EXACT>(dp, reinterpret_cast<const int *>(J->mem + J->pl.off_zero),
+                           reinterpret_cast<const SweepItem *>(J->mem + J->pl.off_items), J->pl.nitems, par, s, st);
+    ctx->launches += 1;
+    return;
+  }
+  Params<T> &p = cells<T>(J)[par];
   if (J->d.mode == OIDT_MODE_YEE3D) {
     dim3 blk(kBlock3Z, kBlock3Y), grd((p.nz + kBlock3Z - 1) / kBlock3Z, (p.ny + kBlock3Y - 1) / kBlock3Y, p.nx);
     k_y3_e<T, EXACT><<<grd, blk, 0, st>>>(p, s);
@@ -504,35 +678,41 @@ template <typename T, bool EXACT> void launch_fold(oidt_ctx *ctx, Job *J, int co
   const int wi = J->d.mode == OIDT_MODE_YEE3D ? fp.whi0 - fp.wlo0 : 1;
   dim3 grd((wi * wj + 127) / 128, (fp.nf + kFoldF - 1) / kFoldF, 2 * fp.ncomp);
   k_fold<T, EXACT><<<grd, 128, 0, st>>>(fp, count);
-  k_bump<<<1, 32, 0, st>>>(params_of<T>(J).state, count);
+  k_bump<<<1, 32, 0, st>>>(reinterpret_cast<int *>(J->mem + J->pl.off_state), count);
   ctx->launches += 2;
 }
+
+int steps_flip(const Job *J) { return J->pl.variant == kVariantSweep ? 1 : 0; }
 
 template <typename T, bool EXACT> int advance_t(oidt_ctx *ctx, Job *J, int nsteps) {
   cudaStream_t st = ctx->stream;
   CU(ctx, cudaStreamWaitEvent(st, J->ready, 0));
   const int K = J->pl.K;
+  const int flip = steps_flip(J);
   int left = nsteps;
   while (left > 0) {
     const int cnt = std::min(K, left);
+    const int par = J->parity;
     if (cnt == K) {
-      if (!J->graph) {
+      if (!J->graph[par]) {
         cudaGraph_t g;
+        const long long before = ctx->launches;
         CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        long long before = ctx->launches;
-        for (int s = 0; s < K; ++s) launch_step<T, EXACT>(ctx, J, s, st);
+        for (int s = 0; s < K; ++s) launch_step<T, EXACT>(ctx, J, s, par ^ (flip & s), st);
         launch_fold<T, EXACT>(ctx, J, K, st);
-        ctx->launches = before;  // counted at replay
         CU(ctx, cudaStreamEndCapture(st, &g));
-        CU(ctx, cudaGraphInstantiate(&J->graph, g, 0));
+        CU(ctx, cudaGraphInstantiate(&J->graph[par], g, 0));
         CU(ctx, cudaGraphDestroy(g));
+        J->graph_launches = ctx->launches - before;
+        ctx->launches = before;
       }
-      CU(ctx, cudaGraphLaunch(J->graph, st));
-      ctx->launches += 2 * K + 2;
+      CU(ctx, cudaGraphLaunch(J->graph[par], st));
+      ctx->launches += J->graph_launches;
     } else {
-      for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, st);
+      for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, par ^ (flip & s), st);
       launch_fold<T, EXACT>(ctx, J, cnt, st);
     }
+    J->parity ^= flip & cnt;
     left -= cnt;
   }
   CU(ctx, cudaGetLastError());
@@ -549,77 +729,122 @@ int advance(oidt_ctx *ctx, Job *J, int nsteps) {
 }
 
 // ---- multi-job launches ----------------------------------------------------
-std::vector<Tile> make_tiles(const std::vector<Job *> &js) {
-  std::vector<Tile> t;
+void drop_batch(BatchPlan &bp) {
+  if (bp.graph) cudaGraphExecDestroy(bp.graph);
+  bp.graph = nullptr;
+  if (bp.mem) cudaFree(bp.mem);
+  bp.mem = nullptr;
+  bp.ids.clear();
+  bp.pars.clear();
+}
+
+template <typename T, bool EXACT>
+int batch_plan(oidt_ctx *ctx, std::vector<Job *> &js) {
+  BatchPlan &bp = ctx->batch;
+  std::vector<uint64_t> ids;
+  std::vector<int> pars;
+  for (Job *j : js) ids.push_back(j->id), pars.push_back(j->parity);
+  if (bp.mem && bp.ids == ids && bp.pars == pars && bp.K == js[0]->pl.K) return OIDT_OK;
+  drop_batch(bp);
+  std::vector<Tile> tiles;
+  std::vector<SweepItem> items;
+  std::vector<Params<T>> pcell, pview;
+  std::vector<int> par0;
   for (int b = 0; b < (int)js.size(); ++b) {
-    const oidt_job_desc &d = js[b]->d;
-    if (d.mode == OIDT_MODE_YEE3D) {
+    Job *J = js[b];
+    const oidt_job_desc &d = J->d;
+    pcell.push_back(cells<T>(J)[J->parity]);
+    pview.push_back(views<T>(J)[0]);
+    pview.push_back(views<T>(J)[1]);
+    par0.push_back(J->parity);
+    if (J->pl.variant == kVariantSweep) {
+      std::vector<SweepItem> it = sweep_items(&d, J->pl.L, b);
+      items.insert(items.end(), it.begin(), it.end());
+    } else if (d.mode == OIDT_MODE_YEE3D) {
       for (int i = 0; i < d.nx; ++i)
         for (int j0 = 0; j0 < d.ny; j0 += kBlock3Y)
-          for (int k0 = 0; k0 < d.nz; k0 += kBlock3Z) t.push_back({b, i, j0, k0});
+          for (int k0 = 0; k0 < d.nz; k0 += kBlock3Z) tiles.push_back({b, i, j0, k0});
     } else {
       for (int i = 0; i < d.nx; ++i)
-        for (int j0 = 0; j0 < d.ny; j0 += kBlock2) t.push_back({b, i, j0, 0});
+        for (int j0 = 0; j0 < d.ny; j0 += kBlock2) tiles.push_back({b, i, j0, 0});
     }
   }
-  return t;
+  Layout L;
+  const size_t o_t = L.take(tiles.size() * sizeof(Tile) + 16), o_i = L.take(items.size() * sizeof(SweepItem) + 16);
+  const size_t o_c = L.take(pcell.size() * sizeof(Params<T>)), o_v = L.take(pview.size() * sizeof(Params<T>));
+  const size_t o_p = L.take(par0.size() * sizeof(int));
+  CU(ctx, cudaMalloc(&bp.mem, L.off));
+  CU(ctx, cudaMemcpy(bp.mem + o_t, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  CU(ctx, cudaMemcpy(bp.mem + o_i, items.data(), items.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
+  CU(ctx, cudaMemcpy(bp.mem + o_c, pcell.data(), pcell.size() * sizeof(Params<T>), cudaMemcpyHostToDevice));
+  CU(ctx, cudaMemcpy(bp.mem + o_v, pview.data(), pview.size() * sizeof(Params<T>), cudaMemcpyHostToDevice));
+  CU(ctx, cudaMemcpy(bp.mem + o_p, par0.data(), par0.size() * sizeof(int), cudaMemcpyHostToDevice));
+  bp.tiles = reinterpret_cast<Tile *>(bp.mem + o_t);
+  bp.items = reinterpret_cast<SweepItem *>(bp.mem + o_i);
+  bp.pcell = bp.mem + o_c;
+  bp.pview = bp.mem + o_v;
+  bp.par0 = reinterpret_cast<int *>(bp.mem + o_p);
+  bp.ntiles = (int)tiles.size();
+  bp.nitems = (int)items.size();
+  bp.ids = ids;
+  bp.pars = pars;
+  bp.K = js[0]->pl.K;
+  return OIDT_OK;
+}
+
+// s-th step of a block for every job of the plan: sweep jobs launch-step
+// parity s & 1 relative to their parity at plan time; per-cell jobs run in
+// place on their current buffer.
+template <typename T, bool EXACT> void batch_block(oidt_ctx *ctx, std::vector<Job *> &js, int cnt, cudaStream_t st) {
+  BatchPlan &bp = ctx->batch;
+  const Params<T> *dc = reinterpret_cast<const Params<T> *>(bp.pcell);
+  const Params<T> *dv = reinterpret_cast<const Params<T> *>(bp.pview);
+  for (int s = 0; s < cnt; ++s) {
+    if (bp.nitems) {
+      launch_sweep<T, EXACT>(dv, bp.par0, bp.items, bp.nitems, s & 1, s, st);
+      ctx->launches += 1;
+    }
+    if (bp.ntiles) {
+      k_batch<T, EXACT, true><<<bp.ntiles, 128, 0, st>>>(dc, bp.tiles, s);
+      k_batch<T, EXACT, false><<<bp.ntiles, 128, 0, st>>>(dc, bp.tiles, s);
+      ctx->launches += 2;
+    }
+  }
+  for (Job *j : js) launch_fold<T, EXACT>(ctx, j, cnt, st);
 }
 
 template <typename T, bool EXACT>
 int batch_t(oidt_ctx *ctx, std::vector<Job *> &js, int nsteps) {
   cudaStream_t st = ctx->stream;
-  BatchPlan &bp = ctx->batch;
-  std::vector<uint64_t> ids;
-  for (Job *j : js) ids.push_back(j->id);
   const int K = js[0]->pl.K;
   for (Job *j : js) {
     if (j->pl.K != K) return fail(ctx, OIDT_ERR_INVALID, "batched jobs must share ring_steps");
     CU(ctx, cudaStreamWaitEvent(st, j->ready, 0));
   }
-  if (bp.ids != ids || bp.K != K) {
-    if (bp.graph) { cudaGraphExecDestroy(bp.graph); bp.graph = nullptr; }
-    if (bp.tiles) { cudaFree(bp.tiles); bp.tiles = nullptr; }
-    std::vector<Tile> t = make_tiles(js);
-    // Params of job b must sit at params[b]: gather them into one array.
-    CU(ctx, cudaMalloc(&bp.tiles, t.size() * sizeof(Tile) + js.size() * sizeof(Params<T>) + 256));
-    CU(ctx, cudaMemcpy(bp.tiles, t.data(), t.size() * sizeof(Tile), cudaMemcpyHostToDevice));
-    Params<T> *dp = reinterpret_cast<Params<T> *>(reinterpret_cast<unsigned char *>(bp.tiles) +
-                                                  align_up(t.size() * sizeof(Tile)));
-    std::vector<Params<T>> hp;
-    for (Job *j : js) hp.push_back(params_of<T>(j));
-    CU(ctx, cudaMemcpy(dp, hp.data(), hp.size() * sizeof(Params<T>), cudaMemcpyHostToDevice));
-    bp.ntiles = (int)t.size();
-    bp.ids = ids;
-    bp.K = K;
-  }
-  const Params<T> *dp = reinterpret_cast<const Params<T> *>(reinterpret_cast<unsigned char *>(bp.tiles) +
-                                                            align_up(bp.ntiles * sizeof(Tile)));
-  auto block = [&](int cnt) {
-    for (int s = 0; s < cnt; ++s) {
-      k_batch<T, EXACT, true><<<bp.ntiles, 128, 0, st>>>(dp, bp.tiles, s);
-      k_batch<T, EXACT, false><<<bp.ntiles, 128, 0, st>>>(dp, bp.tiles, s);
-    }
-    for (Job *j : js) launch_fold<T, EXACT>(ctx, j, cnt, st);
-    ctx->launches += 2 * cnt;
-  };
   int left = nsteps;
   while (left > 0) {
+    int rc = batch_plan<T, EXACT>(ctx, js);
+    if (rc) return rc;
+    BatchPlan &bp = ctx->batch;
     const int cnt = std::min(K, left);
-    if (cnt == K) {
+    if (cnt == K && (K & 1) == 0) {
       if (!bp.graph) {
         cudaGraph_t g;
-        long long before = ctx->launches;
+        const long long before = ctx->launches;
         CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        block(K);
+        batch_block<T, EXACT>(ctx, js, K, st);
         CU(ctx, cudaStreamEndCapture(st, &g));
+        bp.graph_launches = ctx->launches - before;
         ctx->launches = before;
         CU(ctx, cudaGraphInstantiate(&bp.graph, g, 0));
         CU(ctx, cudaGraphDestroy(g));
       }
       CU(ctx, cudaGraphLaunch(bp.graph, st));
-      ctx->launches += 2 * K + 2 * (long long)js.size();
+      ctx->launches += bp.graph_launches;
     } else {
-      block(cnt);
+      batch_block<T, EXACT>(ctx, js, cnt, st);
+      if (cnt & 1)  // sweep jobs end this block on the other buffer
+        for (Job *j : js) j->parity ^= steps_flip(j);
     }
     left -= cnt;
   }
@@ -651,6 +876,89 @@ int wait_event(oidt_ctx *ctx, cudaEvent_t ev, int timeout_ms) {
   }
 }
 
+template <typename T, bool EXACT> int profile_t(oidt_ctx *ctx, Job *J, int nsteps, float *ms) {
+  cudaStream_t st = ctx->stream;
+  CU(ctx, cudaStreamWaitEvent(st, J->ready, 0));
+  std::vector<cudaEvent_t> ev(2 * (2 * nsteps + 2));
+  for (auto &e : ev) CU(ctx, cudaEventCreate(&e));
+  const bool sweep = J->pl.variant == kVariantSweep;
+  int q = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    const int par = J->parity ^ (sweep ? (s & 1) : 0);
+    if (sweep) {  // one launch per step: reported as the E half, H half = 0
+      cudaEventRecord(ev[q++], st);
+      launch_step<T, EXACT>(ctx, J, s, par, st);
+      cudaEventRecord(ev[q++], st);
+      cudaEventRecord(ev[q++], st);
+      cudaEventRecord(ev[q++], st);
+      continue;
+    }
+    Params<T> &p = cells<T>(J)[par];
+    if (J->d.mode == OIDT_MODE_YEE3D) {
+      dim3 blk(kBlock3Z, kBlock3Y), grd((p.nz + kBlock3Z - 1) / kBlock3Z, (p.ny + kBlock3Y - 1) / kBlock3Y, p.nx);
+      cudaEventRecord(ev[q++], st);
+      k_y3_e<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+      cudaEventRecord(ev[q++], st);
+      cudaEventRecord(ev[q++], st);
+      k_y3_h<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+      cudaEventRecord(ev[q++], st);
+    } else {
+      dim3 blk(kBlock2), grd((p.ny + kBlock2 - 1) / kBlock2, p.nx);
+      cudaEventRecord(ev[q++], st);
+      k_2d_e<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+      cudaEventRecord(ev[q++], st);
+      cudaEventRecord(ev[q++], st);
+      k_2d_h<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+      cudaEventRecord(ev[q++], st);
+    }
+    ctx->launches += 2;
+  }
+  cudaEventRecord(ev[q++], st);
+  launch_fold<T, EXACT>(ctx, J, nsteps, st);
+  cudaEventRecord(ev[q++], st);
+  CU(ctx, cudaGetLastError());
+  CU(ctx, cudaStreamSynchronize(st));
+  double se = 0, sh = 0;
+  for (int s = 0; s < nsteps; ++s) {
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ev[4 * s], ev[4 * s + 1]);
+    cudaEventElapsedTime(&b, ev[4 * s + 2], ev[4 * s + 3]);
+    se += a;
+    sh += b;
+  }
+  float fo = 0;
+  cudaEventElapsedTime(&fo, ev[4 * nsteps], ev[4 * nsteps + 1]);
+  ms[0] = (float)(se / nsteps);
+  ms[1] = (float)(sh / nsteps);
+  ms[2] = fo;
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (sweep) J->parity ^= nsteps & 1;
+  J->steps_enqueued += nsteps;
+  CU(ctx, cudaEventRecord(J->done, st));
+  return OIDT_OK;
+}
+
+void destroy_job(oidt_ctx *ctx, Job *J) {
+  for (int b = 0; b < 2; ++b)
+    if (J->graph[b]) cudaGraphExecDestroy(J->graph[b]);
+  cudaFreeAsync(J->mem, ctx->stream);  // stream-ordered: no device-wide synchronisation
+  cudaEventDestroy(J->ready);
+  cudaEventDestroy(J->done);
+  delete J;
+}
+
+int set_sweep_attrs() {
+  cudaFuncSetAttribute(k_sweep3d<float, false, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<float>());
+  cudaFuncSetAttribute(k_sweep3d<float, true, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<float>());
+  cudaFuncSetAttribute(k_sweep3d<double, false, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<double>());
+  cudaFuncSetAttribute(k_sweep3d<double, true, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<double>());
+  int per_sm = 0, sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep3d<float, false, TY, TZ, ST>, TY * TZ, sweep_smem<float>());
+  return std::max(1, per_sm) * std::max(1, sms);
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -672,6 +980,7 @@ int32_t oidt_create(int32_t device, uint64_t hbm_budget, oidt_ctx **out) {
     delete ctx;
     return OIDT_ERR_CUDA;
   }
+  g_sweep_slots = set_sweep_attrs();
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   ctx->budget = hbm_budget ? hbm_budget : (uint64_t)(0.9 * (double)fr);
@@ -685,17 +994,9 @@ int32_t oidt_destroy(oidt_ctx *ctx) {
     std::lock_guard<std::mutex> g(ctx->mu);
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    for (auto &kv : ctx->jobs) {
-      Job *J = kv.second;
-      if (J->graph) cudaGraphExecDestroy(J->graph);
-      cudaFreeAsync(J->mem, ctx->stream);
-      cudaEventDestroy(J->ready);
-      cudaEventDestroy(J->done);
-      delete J;
-    }
+    for (auto &kv : ctx->jobs) destroy_job(ctx, kv.second);
     ctx->jobs.clear();
-    if (ctx->batch.graph) cudaGraphExecDestroy(ctx->batch.graph);
-    if (ctx->batch.tiles) cudaFree(ctx->batch.tiles);
+    drop_batch(ctx->batch);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
     cudaStreamDestroy(ctx->upload);
@@ -791,6 +1092,8 @@ int32_t oidt_batch_advance(oidt_ctx *ctx, const uint64_t *jobs, int32_t njobs, i
     if (J->steps_enqueued + nsteps > J->d.nt) return fail(ctx, OIDT_ERR_STATE, "job %llu has too few source steps", (unsigned long long)jobs[b]);
     if (!js.empty() && (J->d.precision != js[0]->d.precision || J->d.arith != js[0]->d.arith))
       return fail(ctx, OIDT_ERR_INVALID, "batched jobs must share precision and arithmetic");
+    for (Job *o : js)
+      if (o == J) return fail(ctx, OIDT_ERR_INVALID, "job %llu listed twice", (unsigned long long)jobs[b]);
     js.push_back(J);
   }
   if (nsteps == 0) return OIDT_OK;
@@ -803,12 +1106,14 @@ int32_t oidt_batch_advance(oidt_ctx *ctx, const uint64_t *jobs, int32_t njobs, i
 int32_t oidt_job_sync(oidt_ctx *ctx, uint64_t job, int32_t timeout_ms) {
   if (!ctx) return OIDT_ERR_INVALID;
   cudaEvent_t ev;
+  int *state = nullptr;
   {
     std::lock_guard<std::mutex> g(ctx->mu);
     Job *J = find(ctx, job);
     if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
     if (!J->busy) return OIDT_OK;
     ev = J->done;
+    state = reinterpret_cast<int *>(J->mem + J->pl.off_state);
   }
   cudaSetDevice(ctx->device);
   int rc = wait_event(ctx, ev, timeout_ms);
@@ -816,6 +1121,9 @@ int32_t oidt_job_sync(oidt_ctx *ctx, uint64_t job, int32_t timeout_ms) {
     std::lock_guard<std::mutex> g(ctx->mu);
     Job *J = find(ctx, job);
     if (J && J->done == ev) J->busy = cudaEventQuery(ev) != cudaSuccess;
+    int flags[2] = {0, 0};
+    if (cudaMemcpy(flags, state, sizeof flags, cudaMemcpyDeviceToHost) == cudaSuccess && flags[1])
+      return fail(ctx, OIDT_ERR_TIMEOUT, "a kernel's bounded wait on its tile loads expired (device flag %d)", flags[1]);
   }
   return rc;
 }
@@ -868,12 +1176,11 @@ int32_t oidt_job_read_field(oidt_ctx *ctx, uint64_t job, int32_t field, void *ou
   Job *J = find(ctx, job);
   if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
   if (!field_ok(J, field)) return fail(ctx, OIDT_ERR_INVALID, "field %d not in this solver", field);
-  const size_t need = J->pl.N * J->pl.esz;
+  const size_t need = (size_t)J->d.nx * J->d.ny * J->d.nz * J->pl.esz;
   if (nbytes < need) return fail(ctx, OIDT_ERR_INVALID, "output needs %zu bytes", need);
   int rc = read_common(ctx, J);
   if (rc) return rc;
-  CU(ctx, cudaMemcpy(out, J->mem + J->pl.off_f[field], need, cudaMemcpyDeviceToHost));
-  return OIDT_OK;
+  return copy_grid_d2h(ctx, J, out, J->mem + J->pl.off_f[J->pl.nbuf == 2 ? J->parity : 0][field]);
 }
 
 int32_t oidt_job_write_field(oidt_ctx *ctx, uint64_t job, int32_t field, const void *src, size_t nbytes) {
@@ -882,11 +1189,17 @@ int32_t oidt_job_write_field(oidt_ctx *ctx, uint64_t job, int32_t field, const v
   Job *J = find(ctx, job);
   if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
   if (!field_ok(J, field)) return fail(ctx, OIDT_ERR_INVALID, "field %d not in this solver", field);
-  const size_t need = J->pl.N * J->pl.esz;
+  const size_t need = (size_t)J->d.nx * J->d.ny * J->d.nz * J->pl.esz;
   if (nbytes != need) return fail(ctx, OIDT_ERR_INVALID, "input must be %zu bytes", need);
   int rc = read_common(ctx, J);
   if (rc) return rc;
-  CU(ctx, cudaMemcpy(J->mem + J->pl.off_f[field], src, need, cudaMemcpyHostToDevice));
+  // Both buffers: cells a step never updates (the PEC rim planes) are not
+  // copied between the plane-sweep buffers, so they must agree in both.
+  for (int b = 0; b < J->pl.nbuf; ++b) {
+    rc = copy_grid_h2d(ctx, J, J->mem + J->pl.off_f[b][field], src, ctx->upload);
+    if (rc) return rc;
+  }
+  CU(ctx, cudaStreamSynchronize(ctx->upload));
   return OIDT_OK;
 }
 
@@ -903,7 +1216,8 @@ int32_t oidt_job_read_psi(oidt_ctx *ctx, uint64_t job, int32_t field, int32_t ax
   if (nbytes < need) return fail(ctx, OIDT_ERR_INVALID, "output needs %zu bytes", need);
   int rc = read_common(ctx, J);
   if (rc) return rc;
-  CU(ctx, cudaMemcpy(out, J->mem + J->pl.off_psi[field][axis][side], need, cudaMemcpyDeviceToHost));
+  const int b = (is_e(field) && J->pl.nbuf == 2) ? J->parity : 0;
+  CU(ctx, cudaMemcpy(out, J->mem + J->pl.off_psi[b][field][axis][side], need, cudaMemcpyDeviceToHost));
   return OIDT_OK;
 }
 
@@ -914,19 +1228,56 @@ int32_t oidt_job_release(oidt_ctx *ctx, uint64_t job) {
   if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
   CU(ctx, cudaSetDevice(ctx->device));
   CU(ctx, cudaEventSynchronize(J->done));
-  if (J->graph) cudaGraphExecDestroy(J->graph);
-  if (std::find(ctx->batch.ids.begin(), ctx->batch.ids.end(), job) != ctx->batch.ids.end()) {
-    if (ctx->batch.graph) cudaGraphExecDestroy(ctx->batch.graph);
-    ctx->batch.graph = nullptr;
-    ctx->batch.ids.clear();
-  }
-  cudaFreeAsync(J->mem, ctx->stream);  // stream-ordered: no device-wide synchronisation
-  cudaEventDestroy(J->ready);
-  cudaEventDestroy(J->done);
+  if (std::find(ctx->batch.ids.begin(), ctx->batch.ids.end(), job) != ctx->batch.ids.end()) drop_batch(ctx->batch);
   ctx->in_use -= J->pl.total;
   ctx->jobs.erase(job);
-  delete J;
+  destroy_job(ctx, J);
   return OIDT_OK;
+}
+
+int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
+  if (!ctx) return OIDT_ERR_INVALID;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  Job *J = find(ctx, job);
+  if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
+  CU(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  CU(ctx, cudaStreamWaitEvent(st, J->ready, 0));
+  const JobPlan &pl = J->pl;
+  for (int b = 0; b < pl.nbuf; ++b)
+    for (int f : fields_of(J->d.mode)) CU(ctx, cudaMemsetAsync(J->mem + pl.off_f[b][f], 0, pl.N * pl.esz, st));
+  for (auto fa : psi_pairs(J->d.mode))
+    for (int b = 0; b < (is_e(fa.first) ? pl.nbuf : 1); ++b)
+      for (int sd = 0; sd < 2; ++sd)
+        CU(ctx, cudaMemsetAsync(J->mem + pl.off_psi[b][fa.first][fa.second][sd], 0,
+                                psi_elems(J->d.mode, fa.second, J->d.nx, J->d.ny, J->d.nz, J->d.num_cpml) * pl.esz, st));
+  CU(ctx, cudaMemsetAsync(J->mem + pl.off_ring, 0, pl.off_acc - pl.off_ring, st));
+  CU(ctx, cudaMemsetAsync(J->mem + pl.off_acc, 0, pl.off_state - pl.off_acc, st));
+  CU(ctx, cudaMemsetAsync(J->mem + pl.off_state, 0, 64, st));
+  CU(ctx, cudaEventRecord(J->done, st));
+  J->busy = true;
+  J->steps_enqueued = 0;
+  J->parity = 0;
+  return OIDT_OK;
+}
+
+int32_t oidt_ctx_stream(oidt_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return OIDT_ERR_INVALID;
+  *stream = (void *)ctx->stream;
+  return OIDT_OK;
+}
+
+int32_t oidt_job_profile(oidt_ctx *ctx, uint64_t job, int32_t nsteps, float *ms_out) {
+  if (!ctx || !ms_out || nsteps <= 0) return OIDT_ERR_INVALID;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  Job *J = find(ctx, job);
+  if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
+  if (nsteps > J->pl.K) return fail(ctx, OIDT_ERR_INVALID, "profile at most ring_steps (%d) steps", J->pl.K);
+  if (J->steps_enqueued + nsteps > J->d.nt) return fail(ctx, OIDT_ERR_STATE, "not enough source steps left");
+  CU(ctx, cudaSetDevice(ctx->device));
+  const bool f64 = J->d.precision == OIDT_F64, ex = J->d.arith == OIDT_ARITH_EXACT;
+  if (f64) return ex ? profile_t<double, true>(ctx, J, nsteps, ms_out) : profile_t<double, false>(ctx, J, nsteps, ms_out);
+  return ex ? profile_t<float, true>(ctx, J, nsteps, ms_out) : profile_t<float, false>(ctx, J, nsteps, ms_out);
 }
 
 }  // extern "C"

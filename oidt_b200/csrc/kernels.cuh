@@ -58,14 +58,19 @@ template <> struct Ar<double, false> {
 template <typename T> struct Params {
   int mode;              // OIDT_MODE_*
   int nx, ny, nz;        // nz = 1 in 2D
+  int nzp;               // 3D row pitch along z (elements); 2D: 1
   int P, ib, jb, kb, ie, je, ke;
-  T *f[6];               // fields, reference layout
+  T *f[6];               // fields (read; updated in place by the per-cell launches)
+  T *fn[6];              // fields written by the plane sweep (the other buffer)
   const T *cb[3];        // dt/eps per E component (TM2 uses cb[2] for Ez)
   const T *kd[6];        // kappa*dx: kxe kye kze kxh kyh kzh
   const T *rkd[6];       // reciprocals
   const T *be, *ce, *bh, *ch;
   T db, dx, rdx;
-  T *psi[6][3][2];       // [field][slab axis][side]
+  T *psi[6][3][2];       // [field][slab axis][side] (read; H psi updated in place)
+  T *psin[6][3][2];      // E psi written (== psi for the per-cell launches)
+  const void *tmap_f;    // plane sweep: 6 CUtensorMaps of f[] (device memory)
+  const void *tmap_cb;   // plane sweep: 3 CUtensorMaps of cb[]
   int src_field;         // -1: none
   int slo[3], shi[3];
   const T *jsrc;
@@ -115,111 +120,138 @@ __device__ __forceinline__ void capture(const Params<T> &p, int s, int port, int
 
 // ---------------------------------------------------------------------------
 // 3D Yee (FDTD/GPU/FDTD_3D/s-parameter_extraction/fdtd_funcs.py)
+//
+// The arithmetic of one cell lives in y3_e_compute / y3_h_compute, written
+// against an accessor: the per-cell launch reads neighbours from global
+// memory (GlobalAcc3), the plane-sweep kernel from shared-memory tiles.  Both
+// therefore perform the identical operation sequence.
+// Accessor interface:
+//   h(f, di, dj, dk)   old H component f at (i+di, j+dj, k+dk), di,dj,dk in {0,1}
+//   e(f, di, dj, dk)   new E component f at (i+di, j+dj, k+dk), offsets in {-1,0}
+//   eold(f), hold(f), cb(a)
 // ---------------------------------------------------------------------------
-template <typename T, bool EXACT>
-__device__ __forceinline__ void y3_e_cell(const Params<T> &p, int i, int j, int k, int n, int s) {
+template <typename T> struct GlobalAcc3 {
+  const Params<T> &p;
+  long long c, sy, sx;
+  __device__ __forceinline__ T h(int f, int di, int dj, int dk) const { return p.f[f][c + di * sx + dj * sy + dk]; }
+  __device__ __forceinline__ T e(int f, int di, int dj, int dk) const { return p.f[f][c + di * sx + dj * sy + dk]; }
+  __device__ __forceinline__ T eold(int f) const { return p.f[f][c]; }
+  __device__ __forceinline__ T hold(int f) const { return p.f[f][c]; }
+  __device__ __forceinline__ T cb(int a) const { return p.cb[a][c]; }
+};
+
+// New E at cell (i, j, k) -> out[EX..EZ] (old value where a component is not
+// updated).  own: write the new CPML psi (else only read it: halo cells of a
+// sweep tile).  Returns a bit mask of the updated components.
+template <typename T, bool EXACT, class Acc>
+__device__ __forceinline__ int y3_e_compute(const Params<T> &p, const Acc &a, int i, int j, int k, int n, bool own,
+                                            T out[3]) {
   using A = Ar<T, EXACT>;
   const int nx = p.nx, ny = p.ny, nz = p.nz, P = p.P;
-  const long long sy = nz, sx = (long long)ny * nz;
-  const long long c = i * sx + j * sy + k;
-  const T *Hx = p.f[HX], *Hy = p.f[HY], *Hz = p.f[HZ];
   const T Jn = p.src_field >= 0 ? p.jsrc[n] : T(0);
-  int d, side, q;
+  int d, side, q, mask = 0;
+  out[0] = a.eold(EX);
+  out[1] = a.eold(EY);
+  out[2] = a.eold(EZ);
   // Ex: i in (ib, ie), j in [jb, je), k in [kb, ke)         :43-50
   if (i > p.ib && i < p.ie && j >= p.jb && j < p.je && k >= p.kb && k < p.ke) {
-    const T cb = p.cb[0][c];
-    const T dhz = A::sub(Hz[c + sy], Hz[c]);
-    const T dhy = A::sub(Hy[c + 1], Hy[c]);
-    T e = A::add(p.f[EX][c], A::mul(cb, A::sub(A::div(dhz, p.kd[1][j], p.rkd[1][j]),
-                                                A::div(dhy, p.kd[2][k], p.rkd[2][k]))));
+    const T cb = a.cb(0);
+    const T dhz = A::sub(a.h(HZ, 0, 1, 0), a.h(HZ, 0, 0, 0));
+    const T hy1 = a.h(HY, 0, 0, 1), hy0 = a.h(HY, 0, 0, 0);
+    const T dhy = A::sub(hy1, hy0);
+    T e = A::add(out[0], A::mul(cb, A::sub(A::div(dhz, p.kd[1][j], p.rkd[1][j]),
+                                            A::div(dhy, p.kd[2][k], p.rkd[2][k]))));
     if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc :113-123
-      T *ps = p.psi[EX][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
-      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
-      *ps = v;
+      const long long o = psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], p.psi[EX][AY][side][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
+      if (own) p.psin[EX][AY][side][o] = v;
       e = A::add(e, A::mul(cb, v));
     }
     if ((q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ex_zinc :126-136
-      T hy1 = Hy[c + 1], hy0 = Hy[c];
-      if (p.src_field == HY) {  // the Hy source lands between the E curl and E-CPML
-        if (in_src(p, HY, i, j, k + 1)) hy1 = A::sub(hy1, Jn);
-        if (in_src(p, HY, i, j, k)) hy0 = A::sub(hy0, Jn);
+      T h1 = hy1, h0 = hy0;
+      if (p.src_field == HY) {  // the Hy source lands between the E curl and the E-CPML
+        if (in_src(p, HY, i, j, k + 1)) h1 = A::sub(h1, Jn);
+        if (in_src(p, HY, i, j, k)) h0 = A::sub(h0, Jn);
       }
-      T *ps = p.psi[EX][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
-      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], A::sub(hy1, hy0)), p.dx, p.rdx));
-      *ps = v;
+      const long long o = psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], p.psi[EX][AZ][side][o]), A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
+      if (own) p.psin[EX][AZ][side][o] = v;
       e = A::sub(e, A::mul(cb, v));
     }
-    p.f[EX][c] = e;
-    if (k == p.port_pos[0]) capture(p, s, 0, 0, (long long)i * ny + j, e);
-    if (k == p.port_pos[1]) capture(p, s, 1, 0, (long long)i * ny + j, e);
+    out[0] = e;
+    mask |= 1;
   }
   // Ey: i in [ib, ie), j in (jb, je), k in [kb, ke)         :53-60
   if (i >= p.ib && i < p.ie && j > p.jb && j < p.je && k >= p.kb && k < p.ke) {
-    const T cb = p.cb[1][c];
-    const T dhx = A::sub(Hx[c + 1], Hx[c]);
-    const T dhz = A::sub(Hz[c + sx], Hz[c]);
-    T e = A::add(p.f[EY][c], A::mul(cb, A::sub(A::div(dhx, p.kd[2][k], p.rkd[2][k]),
-                                                A::div(dhz, p.kd[0][i], p.rkd[0][i]))));
+    const T cb = a.cb(1);
+    const T dhx = A::sub(a.h(HX, 0, 0, 1), a.h(HX, 0, 0, 0));
+    const T dhz = A::sub(a.h(HZ, 1, 0, 0), a.h(HZ, 0, 0, 0));
+    T e = A::add(out[1], A::mul(cb, A::sub(A::div(dhx, p.kd[2][k], p.rkd[2][k]),
+                                            A::div(dhz, p.kd[0][i], p.rkd[0][i]))));
     if (in_src(p, EY, i, j, k)) e = A::sub(e, Jn);       // update_source :104-110
     if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc :139-149
-      T *ps = p.psi[EY][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
-      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
-      *ps = v;
+      const long long o = psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], p.psi[EY][AX][side][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
+      if (own) p.psin[EY][AX][side][o] = v;
       e = A::sub(e, A::mul(cb, v));
     }
     if ((q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ey_zinc :152-162
-      T *ps = p.psi[EY][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
-      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
-      *ps = v;
+      const long long o = psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], p.psi[EY][AZ][side][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
+      if (own) p.psin[EY][AZ][side][o] = v;
       e = A::add(e, A::mul(cb, v));
     }
-    p.f[EY][c] = e;
-    if (k == p.port_pos[0]) capture(p, s, 0, 1, (long long)i * ny + j, e);
-    if (k == p.port_pos[1]) capture(p, s, 1, 1, (long long)i * ny + j, e);
+    out[1] = e;
+    mask |= 2;
   }
   // Ez: i in [ib, ie), j in [jb, je), k in (kb, ke)         :63-70
   if (i >= p.ib && i < p.ie && j >= p.jb && j < p.je && k > p.kb && k < p.ke) {
-    const T cb = p.cb[2][c];
-    const T dhy = A::sub(Hy[c + sx], Hy[c]);
-    const T dhx = A::sub(Hx[c + sy], Hx[c]);
-    T e = A::add(p.f[EZ][c], A::mul(cb, A::sub(A::div(dhy, p.kd[0][i], p.rkd[0][i]),
-                                                A::div(dhx, p.kd[1][j], p.rkd[1][j]))));
+    const T cb = a.cb(2);
+    const T hy1 = a.h(HY, 1, 0, 0), hy0 = a.h(HY, 0, 0, 0);
+    const T dhy = A::sub(hy1, hy0);
+    const T dhx = A::sub(a.h(HX, 0, 1, 0), a.h(HX, 0, 0, 0));
+    T e = A::add(out[2], A::mul(cb, A::sub(A::div(dhy, p.kd[0][i], p.rkd[0][i]),
+                                            A::div(dhx, p.kd[1][j], p.rkd[1][j]))));
     if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ez_xinc :165-175
-      T hy1 = Hy[c + sx], hy0 = Hy[c];
+      T h1 = hy1, h0 = hy0;
       if (p.src_field == HY) {
-        if (in_src(p, HY, i + 1, j, k)) hy1 = A::sub(hy1, Jn);
-        if (in_src(p, HY, i, j, k)) hy0 = A::sub(hy0, Jn);
+        if (in_src(p, HY, i + 1, j, k)) h1 = A::sub(h1, Jn);
+        if (in_src(p, HY, i, j, k)) h0 = A::sub(h0, Jn);
       }
-      T *ps = p.psi[EZ][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
-      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], A::sub(hy1, hy0)), p.dx, p.rdx));
-      *ps = v;
+      const long long o = psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], p.psi[EZ][AX][side][o]), A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
+      if (own) p.psin[EZ][AX][side][o] = v;
       e = A::add(e, A::mul(cb, v));
     }
     if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ez_yinc :178-188
-      T *ps = p.psi[EZ][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
-      T v = A::add(A::mul(p.be[q], *ps), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
-      *ps = v;
+      const long long o = psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T v = A::add(A::mul(p.be[q], p.psi[EZ][AY][side][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
+      if (own) p.psin[EZ][AY][side][o] = v;
       e = A::sub(e, A::mul(cb, v));
     }
-    p.f[EZ][c] = e;
+    out[2] = e;
+    mask |= 4;
   }
+  return mask;
 }
 
-template <typename T, bool EXACT>
-__device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int k, int n, int s) {
+// New H at cell (i, j, k) -> out[0..2] = Hx, Hy, Hz; CPML psi of H is owned by
+// the cell and updated in place.
+template <typename T, bool EXACT, class Acc>
+__device__ __forceinline__ int y3_h_compute(const Params<T> &p, const Acc &a, int i, int j, int k, int n, T out[3]) {
   using A = Ar<T, EXACT>;
   const int nx = p.nx, ny = p.ny, nz = p.nz, P = p.P;
-  const long long sy = nz, sx = (long long)ny * nz;
-  const long long c = i * sx + j * sy + k;
-  const T *Ex = p.f[EX], *Ey = p.f[EY], *Ez = p.f[EZ];
   const T db = p.db;
-  int d, side, q;
+  int d, side, q, mask = 0;
+  out[0] = a.hold(HX);
+  out[1] = a.hold(HY);
+  out[2] = a.hold(HZ);
   // Hx: i in [ib, ie), j in (jb, je), k in (kb, ke)         :73-80
   if (i >= p.ib && i < p.ie && j > p.jb && j < p.je && k > p.kb && k < p.ke) {
-    const T dey = A::sub(Ey[c], Ey[c - 1]);
-    const T dez = A::sub(Ez[c], Ez[c - sy]);
-    T h = A::add(p.f[HX][c], A::mul(db, A::sub(A::div(dey, p.kd[5][k], p.rkd[5][k]),
-                                                A::div(dez, p.kd[4][j], p.rkd[4][j]))));
+    const T dey = A::sub(a.e(EY, 0, 0, 0), a.e(EY, 0, 0, -1));
+    const T dez = A::sub(a.e(EZ, 0, 0, 0), a.e(EZ, 0, -1, 0));
+    T h = A::add(out[0], A::mul(db, A::sub(A::div(dey, p.kd[5][k], p.rkd[5][k]),
+                                            A::div(dez, p.kd[4][j], p.rkd[4][j]))));
     if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc :191-201
       T *ps = p.psi[HX][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
@@ -232,17 +264,14 @@ __device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int 
       *ps = v;
       h = A::add(h, A::mul(db, v));
     }
-    p.f[HX][c] = h;
-    if (k == p.port_pos[0]) capture(p, s, 0, 2, (long long)i * ny + j, h);
-    if (k == p.port_pos[1]) capture(p, s, 1, 2, (long long)i * ny + j, h);
-    if (k == p.port_pos[0] + 1) capture(p, s, 0, 3, (long long)i * ny + j, h);
-    if (k == p.port_pos[1] + 1) capture(p, s, 1, 3, (long long)i * ny + j, h);
+    out[0] = h;
+    mask |= 1;
   }
   // Hy: i in (ib, ie), j in [jb, je), k in (kb, ke)         :83-90
   if (i > p.ib && i < p.ie && j >= p.jb && j < p.je && k > p.kb && k < p.ke) {
-    const T dez = A::sub(Ez[c], Ez[c - sx]);
-    const T dex = A::sub(Ex[c], Ex[c - 1]);
-    T h = p.f[HY][c];
+    const T dez = A::sub(a.e(EZ, 0, 0, 0), a.e(EZ, -1, 0, 0));
+    const T dex = A::sub(a.e(EX, 0, 0, 0), a.e(EX, 0, 0, -1));
+    T h = out[1];
     if (in_src(p, HY, i, j, k)) h = A::sub(h, p.jsrc[n]);  // source precedes update_hy
     h = A::add(h, A::mul(db, A::sub(A::div(dez, p.kd[3][i], p.rkd[3][i]),
                                      A::div(dex, p.kd[5][k], p.rkd[5][k]))));
@@ -258,18 +287,15 @@ __device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int 
       *ps = v;
       h = A::sub(h, A::mul(db, v));
     }
-    p.f[HY][c] = h;
-    if (k == p.port_pos[0]) capture(p, s, 0, 4, (long long)i * ny + j, h);
-    if (k == p.port_pos[1]) capture(p, s, 1, 4, (long long)i * ny + j, h);
-    if (k == p.port_pos[0] + 1) capture(p, s, 0, 5, (long long)i * ny + j, h);
-    if (k == p.port_pos[1] + 1) capture(p, s, 1, 5, (long long)i * ny + j, h);
+    out[1] = h;
+    mask |= 2;
   }
   // Hz: i in (ib, ie), j in (jb, je), k in [kb, ke)         :93-100
   if (i > p.ib && i < p.ie && j > p.jb && j < p.je && k >= p.kb && k < p.ke) {
-    const T dex = A::sub(Ex[c], Ex[c - sy]);
-    const T dey = A::sub(Ey[c], Ey[c - sx]);
-    T h = A::add(p.f[HZ][c], A::mul(db, A::sub(A::div(dex, p.kd[4][j], p.rkd[4][j]),
-                                                A::div(dey, p.kd[3][i], p.rkd[3][i]))));
+    const T dex = A::sub(a.e(EX, 0, 0, 0), a.e(EX, 0, -1, 0));
+    const T dey = A::sub(a.e(EY, 0, 0, 0), a.e(EY, -1, 0, 0));
+    T h = A::add(out[2], A::mul(db, A::sub(A::div(dex, p.kd[4][j], p.rkd[4][j]),
+                                            A::div(dey, p.kd[3][i], p.rkd[3][i]))));
     if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hz_xinc :243-253
       T *ps = p.psi[HZ][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
@@ -282,8 +308,63 @@ __device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int 
       *ps = v;
       h = A::add(h, A::mul(db, v));
     }
-    p.f[HZ][c] = h;
+    out[2] = h;
+    mask |= 4;
   }
+  return mask;
+}
+
+// Port-plane capture of the raw samples the DFT fold colocates (3D slots:
+// 0 Ex(kc) 1 Ey(kc) 2 Hx(kc) 3 Hx(kc+1) 4 Hy(kc) 5 Hy(kc+1)).
+template <typename T>
+__device__ __forceinline__ void y3_capture_e(const Params<T> &p, int s, int i, int j, int k, int mask, const T e[3]) {
+  const long long pc = (long long)i * p.ny + j;
+  for (int q = 0; q < 2; ++q)
+    if (k == p.port_pos[q]) {
+      if (mask & 1) capture(p, s, q, 0, pc, e[0]);
+      if (mask & 2) capture(p, s, q, 1, pc, e[1]);
+    }
+}
+template <typename T>
+__device__ __forceinline__ void y3_capture_h(const Params<T> &p, int s, int i, int j, int k, int mask, const T h[3]) {
+  const long long pc = (long long)i * p.ny + j;
+  for (int q = 0; q < 2; ++q) {
+    if (k == p.port_pos[q]) {
+      if (mask & 1) capture(p, s, q, 2, pc, h[0]);
+      if (mask & 2) capture(p, s, q, 4, pc, h[1]);
+    }
+    if (k == p.port_pos[q] + 1) {
+      if (mask & 1) capture(p, s, q, 3, pc, h[0]);
+      if (mask & 2) capture(p, s, q, 5, pc, h[1]);
+    }
+  }
+}
+
+// Per-cell launches (in place): E half then H half.
+template <typename T, bool EXACT>
+__device__ __forceinline__ void y3_e_cell(const Params<T> &p, int i, int j, int k, int n, int s) {
+  const long long sy = p.nzp, sx = (long long)p.ny * p.nzp;
+  const long long c = i * sx + j * sy + k;
+  GlobalAcc3<T> a{p, c, sy, sx};
+  T e[3];
+  const int m = y3_e_compute<T, EXACT>(p, a, i, j, k, n, true, e);
+  if (m & 1) p.f[EX][c] = e[0];
+  if (m & 2) p.f[EY][c] = e[1];
+  if (m & 4) p.f[EZ][c] = e[2];
+  y3_capture_e(p, s, i, j, k, m, e);
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int k, int n, int s) {
+  const long long sy = p.nzp, sx = (long long)p.ny * p.nzp;
+  const long long c = i * sx + j * sy + k;
+  GlobalAcc3<T> a{p, c, sy, sx};
+  T h[3];
+  const int m = y3_h_compute<T, EXACT>(p, a, i, j, k, n, h);
+  if (m & 1) p.f[HX][c] = h[0];
+  if (m & 2) p.f[HY][c] = h[1];
+  if (m & 4) p.f[HZ][c] = h[2];
+  y3_capture_h(p, s, i, j, k, m, h);
 }
 
 // ---------------------------------------------------------------------------

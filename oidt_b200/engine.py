@@ -21,7 +21,7 @@ OK, ERR_INVALID, ERR_CUDA, ERR_BUDGET, ERR_NOTFOUND, ERR_TIMEOUT, ERR_STATE = 0,
 EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error", "oidt_stats_get",
            "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
            "oidt_job_query", "oidt_job_read_dft", "oidt_job_read_field", "oidt_job_write_field",
-           "oidt_job_read_psi", "oidt_job_release")
+           "oidt_job_read_psi", "oidt_job_release", "oidt_job_reset", "oidt_ctx_stream", "oidt_job_profile")
 
 
 class OidtError(RuntimeError):
@@ -74,6 +74,9 @@ def load_library(path: str = LIB_PATH):
             "oidt_job_write_field": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_read_psi": ([vp, u64, i32, i32, i32, vp, C.c_size_t], i32),
             "oidt_job_release": ([vp, u64], i32),
+            "oidt_job_reset": ([vp, u64], i32),
+            "oidt_ctx_stream": ([vp, C.POINTER(vp)], i32),
+            "oidt_job_profile": ([vp, u64, i32, C.POINTER(C.c_float)], i32),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -126,12 +129,19 @@ class Engine:
         self._check(self.lib.oidt_job_bytes(C.byref(d), C.byref(b)))
         return b.value
 
-    def submit(self, spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0) -> "Job":
-        d, keep = to_desc(spec, arith=arith, precision=precision, ring_steps=ring_steps)
+    def submit(self, spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0,
+               variant: str = "sweep") -> "Job":
+        d, keep = to_desc(spec, arith=arith, precision=precision, ring_steps=ring_steps, variant=variant)
         jid = C.c_uint64()
         self._check(self.lib.oidt_job_create(self.ctx, C.byref(d), C.byref(jid)))
         del keep
         return Job(self, jid.value, spec, np.dtype(precision if precision is not None else spec.precision))
+
+    def stream_handle(self) -> int:
+        """The compute stream (cudaStream_t as an integer)."""
+        h = C.c_void_p()
+        self._check(self.lib.oidt_ctx_stream(self.ctx, C.byref(h)))
+        return h.value or 0
 
     def batch_advance(self, jobs, nsteps: int):
         ids = (C.c_uint64 * len(jobs))(*[j.id for j in jobs])
@@ -197,6 +207,20 @@ class Job:
 
     def fields(self) -> dict:
         return {f: self.field(f) for f in FIELDS[self.spec.mode]}
+
+    def reset(self):
+        """Back to step 0 with coefficients kept on the device."""
+        self.eng._check(self.eng.lib.oidt_job_reset(self.eng.ctx, self.id))
+        self.steps = 0
+        return self
+
+    def profile(self, nsteps: int):
+        """Average per-launch device ms of (E half, H half, DFT fold) over
+        ``nsteps`` un-graphed steps."""
+        ms = (C.c_float * 3)()
+        self.eng._check(self.eng.lib.oidt_job_profile(self.eng.ctx, self.id, nsteps, ms))
+        self.steps += nsteps
+        return tuple(float(v) for v in ms)
 
     def release(self):
         if not self.released:

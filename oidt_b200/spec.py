@@ -84,9 +84,16 @@ class JobDesc(C.Structure):
     ]
 
 
-def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0):
+VARIANTS = {"sweep": 0, "cell": 1}
+
+
+def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "sweep"):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
-    ``keepalive`` must outlive the ``oidt_job_create`` call."""
+    ``keepalive`` must outlive the ``oidt_job_create`` call.
+
+    ``variant`` (3D only): 'sweep' -- one plane-sweep launch per step (E and
+    H fused, TMA-staged tiles); 'cell' -- the per-cell E-half / H-half
+    launches.  2D jobs always use the per-cell launches."""
     prec = np.dtype(precision if precision is not None else spec.precision)
     if prec not in (np.dtype(np.float32), np.dtype(np.float64)):
         raise ValueError("precision must be float32 or float64")
@@ -132,4 +139,5 @@ def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int 
     tw = [arr(t, np.float64) for t in spec.twiddles]
     d.cos_e, d.sin_e, d.cos_h, d.sin_h = tw
     d.ring_steps = ring_steps
+    d.reserved[0] = VARIANTS[variant]
     return d, keep

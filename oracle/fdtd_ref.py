@@ -889,3 +889,16 @@ def dft_complex(s, port, comp):
     else:
         key = ("E", "H")[comp] + p
     return s.dft[key + "r"] + 1j * s.dft[key + "i"]
+
+
+FIELD_BY_ID = {0: "EX", 1: "EY", 2: "EZ", 3: "HX", 4: "HY", 5: "HZ"}
+
+
+def from_spec(spec, dtype=np.float64):
+    """Oracle state from an engine job description (read by attribute: mode,
+    shape, num_cpml, lim_lo/hi, cb, kdx, be/ce/bh/ch, db, dx, src_field id,
+    src_lo/hi, j_src, port_pos, twiddles, nf) -- the same inputs the engine
+    receives, cast to ``dtype``."""
+    return from_arrays(spec.mode, spec.shape, spec.num_cpml, spec.lim_lo, spec.lim_hi, spec.cb, spec.kdx,
+                       spec.be, spec.ce, spec.bh, spec.ch, spec.db, spec.dx, FIELD_BY_ID[spec.src_field],
+                       spec.src_lo, spec.src_hi, spec.j_src, spec.port_pos, spec.twiddles, spec.nf, dtype=dtype)

@@ -8,9 +8,7 @@ FIELD_NAMES = {0: "EX", 1: "EY", 2: "EZ", 3: "HX", 4: "HY", 5: "HZ"}
 
 def oracle_from_spec(spec, dtype=np.float64):
     """Oracle state with the spec's arrays (cast to ``dtype``)."""
-    return R.from_arrays(spec.mode, spec.shape, spec.num_cpml, spec.lim_lo, spec.lim_hi, spec.cb, spec.kdx,
-                         spec.be, spec.ce, spec.bh, spec.ch, spec.db, spec.dx, FIELD_NAMES[spec.src_field],
-                         spec.src_lo, spec.src_hi, spec.j_src, spec.port_pos, spec.twiddles, spec.nf, dtype=dtype)
+    return R.from_spec(spec, dtype)
 
 
 def psi_key(name, axis, side):
