@@ -693,7 +693,7 @@ template <typename T, bool EXACT> int advance_t(oidt_ctx *ctx, Job *J, int nstep
   while (left > 0) {
     const int cnt = std::min(K, left);
     const int par = J->parity;
-    if (cnt == K) {
+    if (cnt == K && J->d.reserved[1] == 0) {
       if (!J->graph[par]) {
         cudaGraph_t g;
         const long long before = ctx->launches;

@@ -114,6 +114,7 @@ __global__ void __launch_bounds__(TY *TZ) k_sweep3d(const Params<T> *__restrict_
         reinterpret_cast<const unsigned long long *>(params + 2 * it.job + ((par ^ par0[it.job]) & 1));
     for (int w = tid; w < (int)(sizeof(Params<T>) / 8); w += NT) sp[w] = src[w];
   }
+  __syncthreads();  // the parameter copy must be complete before any thread reads it
   const Params<T> &p = *reinterpret_cast<const Params<T> *>(sp);
   const int y0 = it.y0, z0 = it.z0, x0 = it.x0, x1 = it.x1;
   const int xs = x0 - 1;          // first plane loaded (E of x0-1 feeds H of x0)
@@ -142,7 +143,6 @@ __global__ void __launch_bounds__(TY *TZ) k_sweep3d(const Params<T> *__restrict_
   };
   __shared__ int s_issued, s_failed;
 
-  __syncthreads();
   if (tid == 0) {
     s_abort = 0;
     for (int k = 0; k < S; ++k) mbar_init(bar + k, 1);

@@ -130,8 +130,9 @@ class Engine:
         return b.value
 
     def submit(self, spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0,
-               variant: str = "sweep") -> "Job":
-        d, keep = to_desc(spec, arith=arith, precision=precision, ring_steps=ring_steps, variant=variant)
+               variant: str = "sweep", graphs: bool = True) -> "Job":
+        d, keep = to_desc(spec, arith=arith, precision=precision, ring_steps=ring_steps, variant=variant,
+                          graphs=graphs)
         jid = C.c_uint64()
         self._check(self.lib.oidt_job_create(self.ctx, C.byref(d), C.byref(jid)))
         del keep

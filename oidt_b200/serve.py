@@ -1,0 +1,146 @@
+"""Continuous-batching request loop for roughness-realization jobs.
+
+Requests (a SimSpec each, or a builder for one) arrive over time.  The loop
+
+1. admits waiting requests in arrival order while the context's HBM budget
+   allows (``oidt_job_create`` refuses with OIDT_ERR_BUDGET otherwise; the
+   request then waits for memory to be freed) -- admission copies the job's
+   coefficients to the device while earlier jobs keep running;
+2. advances every admitted job together by one tick of ``tick`` steps in
+   multi-job launches (``oidt_batch_advance``); jobs with fewer steps left
+   finish on their own in the same stream;
+3. retires finished jobs: reads their port DFTs, computes S11/S21, records
+   latency = finish time - arrival time, frees their memory.
+
+So requests that arrive while others are on the GPU join at the next tick
+and share launches with them; nothing waits for a batch to drain.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .engine import BudgetError, Engine
+from .sparams import forward_s
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float                 # seconds from loop start
+    spec: object                   # SimSpec (reflected / device-under-test run)
+    incident: object = None        # optional SimSpec of the smooth incident run
+    meta: dict = field(default_factory=dict)
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    cells: int
+    steps: int
+    S: dict = None
+    dfts: dict = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+class Server:
+    def __init__(self, engine: Engine, tick: int = 64, precision=np.float32, arith: str = "fast",
+                 keep_dfts: bool = False, ring_steps: int = 32):
+        self.eng = engine
+        self.tick = tick
+        self.precision = precision
+        self.arith = arith
+        self.keep_dfts = keep_dfts
+        self.ring = ring_steps
+        self.active = []   # (request, job[, incident job])
+        self.results = []
+        self.refused = 0
+
+    def _admit(self, req: Request, now: float) -> bool:
+        try:
+            j = self.eng.submit(req.spec, arith=self.arith, precision=self.precision, ring_steps=self.ring)
+        except BudgetError:
+            return False
+        ji = None
+        if req.incident is not None:
+            try:
+                ji = self.eng.submit(req.incident, arith=self.arith, precision=self.precision, ring_steps=self.ring)
+            except BudgetError:
+                j.release()
+                return False
+        self.active.append((req, j, ji, now))
+        return True
+
+    def _retire(self, t0: float):
+        keep = []
+        for (req, j, ji, adm) in self.active:
+            jobs = [x for x in (j, ji) if x is not None]
+            if all(x.steps >= x.spec.nt for x in jobs):
+                for x in jobs:
+                    x.sync()
+                nc = 4 if req.spec.mode == "yee3d" else 2
+                d_ref = {(p, c): j.dft(p, c) for p in (0, 1) for c in range(nc)}
+                d_inc = {(p, c): ji.dft(p, c) for p in (0, 1) for c in range(nc)} if ji is not None else d_ref
+                S = forward_s(req.spec, d_inc, d_ref)
+                fin = time.perf_counter() - t0
+                self.results.append(Result(req.rid, req.arrival, adm, fin, req.spec.ncells, req.spec.nt,
+                                           S={k: v for k, v in S.items() if k != "P_inc"},
+                                           dfts=d_ref if self.keep_dfts else None))
+                for x in jobs:
+                    x.release()
+            else:
+                keep.append((req, j, ji, adm))
+        self.active = keep
+
+    def run(self, requests, realtime: bool = True, max_wall: float = None):
+        """Serve ``requests`` (sorted by arrival).  With ``realtime`` the
+        arrival times are honoured against the wall clock; otherwise every
+        request is available immediately (throughput mode)."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        t0 = time.perf_counter()
+        qi = 0
+        while qi < len(pending) or self.active:
+            now = time.perf_counter() - t0
+            if max_wall is not None and now > max_wall:
+                break
+            # admission: arrived requests, FIFO, while memory allows
+            while qi < len(pending) and (not realtime or pending[qi].arrival <= now):
+                if not self._admit(pending[qi], now):
+                    self.refused += 1
+                    break
+                qi += 1
+            if not self.active:
+                if qi < len(pending) and realtime:
+                    time.sleep(max(0.0, min(0.01, pending[qi].arrival - now)))
+                continue
+            jobs = []
+            for (req, j, ji, adm) in self.active:
+                jobs += [x for x in (j, ji) if x is not None]
+            left = [x.spec.nt - x.steps for x in jobs]
+            full = [x for x, l in zip(jobs, left) if l >= self.tick]
+            rest = [(x, l) for x, l in zip(jobs, left) if 0 < l < self.tick]
+            by_prec = {}
+            for x in full:
+                by_prec.setdefault((str(x.precision)), []).append(x)
+            for group in by_prec.values():
+                self.eng.batch_advance(group, self.tick)
+            for x, l in rest:
+                x.advance(l)
+            if jobs:
+                jobs[0].sync()  # one stream: waiting on any job waits for the tick
+            self._retire(t0)
+        return self.results
+
+
+def latency_stats(results):
+    lat = np.array([r.latency for r in results]) if results else np.zeros(1)
+    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "n": len(results)}
