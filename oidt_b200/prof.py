@@ -1,0 +1,44 @@
+"""Small fixed workloads for profiler captures (ncu launch lists and
+single-kernel captures).
+
+    python -m oidt_b200.prof --workload strip3d --steps 64 [--variant sweep|cell] [--no-graphs]
+
+Runs the named workload for a few hundred launches and exits; the device
+state of the default 3D case (128 x 128 x 256 cells, FP32) is about 0.4 GB,
+so a multi-pass capture of one launch stays small.
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+
+from . import workloads as W
+from .engine import Engine
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="strip3d", choices=("strip3d", "slab2d", "strip3d_large"))
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--variant", default="sweep", choices=("sweep", "cell"))
+    ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--precision", default="float32", choices=("float32", "float64"))
+    a = ap.parse_args(argv)
+    if a.workload == "strip3d":
+        spec = W.strip3d(steps=max(a.steps, 64))
+    elif a.workload == "strip3d_large":
+        spec = W.strip3d(nx=384, ny=384, nz=1024, dx=15e-9, P=16, steps=max(a.steps, 64), core_x_nm=220,
+                         core_y_nm=1000, seed=7)
+    else:
+        spec = W.slab2d(steps=max(a.steps, 64))
+    eng = Engine(0)
+    job = eng.submit(spec, precision=np.dtype(a.precision), variant=a.variant, graphs=not a.no_graphs)
+    job.advance(a.steps).sync()
+    print("ran", a.steps, "steps of", a.workload, spec.shape)
+    job.release()
+    eng.close()
+
+
+if __name__ == "__main__":
+    main()
