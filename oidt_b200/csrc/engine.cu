@@ -44,7 +44,8 @@ constexpr int kDefaultRing = 32;
 constexpr int kFoldF = 8;  // frequencies per fold thread
 constexpr int kBlock3Z = 32, kBlock3Y = 4;
 constexpr int kBlock2 = 128;
-constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;
+constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
+constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread box
 constexpr int kVariantSweep = 0, kVariantCell = 1;
 
 // ---------------------------------------------------------------------------
@@ -79,43 +80,6 @@ __global__ void __launch_bounds__(128) k_2d_h(Params<T> p, int s) {
     tm2_h_cell<T, EXACT>(p, i, j, p.state[0] + s, s);
   else
     te2_h_cell<T, EXACT>(p, i, j, p.state[0] + s, s);
-}
-
-// Multi-job per-cell launch: block b works on tile tiles[b] = {job, i, j0, k0}
-// of the job whose in-place parameters are params[job] (device memory).  3D
-// tiles are 32 (k) x 4 (j) cells of one x-plane, 2D tiles 128 (j) cells.
-struct Tile {
-  int job, i, j0, k0;
-};
-template <typename T, bool EXACT, bool E_HALF>
-__global__ void __launch_bounds__(128) k_batch(const Params<T> *__restrict__ params,
-                                               const Tile *__restrict__ tiles, int s) {
-  static_assert(sizeof(Params<T>) % 8 == 0, "Params must be a whole number of 8-byte words");
-  __shared__ __align__(16) unsigned long long sp[sizeof(Params<T>) / 8];
-  const Tile t = tiles[blockIdx.x];
-  {
-    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(params + t.job);
-    for (int w = threadIdx.x; w < (int)(sizeof(Params<T>) / 8); w += blockDim.x) sp[w] = src[w];
-  }
-  __syncthreads();
-  const Params<T> &p = *reinterpret_cast<const Params<T> *>(sp);
-  const int n = p.state[0] + s;
-  if (p.mode == OIDT_MODE_YEE3D) {
-    const int k = t.k0 + (threadIdx.x & 31), j = t.j0 + (threadIdx.x >> 5);
-    if (k >= p.nz || j >= p.ny) return;
-    if (E_HALF)
-      y3_e_cell<T, EXACT>(p, t.i, j, k, n, s);
-    else
-      y3_h_cell<T, EXACT>(p, t.i, j, k, n, s);
-  } else {
-    const int j = t.j0 + threadIdx.x;
-    if (j >= p.ny) return;
-    if (p.mode == OIDT_MODE_TM2) {
-      if (E_HALF) tm2_e_cell<T, EXACT>(p, t.i, j, n, s); else tm2_h_cell<T, EXACT>(p, t.i, j, n, s);
-    } else {
-      if (E_HALF) te2_e_cell<T, EXACT>(p, t.i, j, n, s); else te2_h_cell<T, EXACT>(p, t.i, j, n, s);
-    }
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -260,18 +224,18 @@ struct JobPlan {
   size_t total;
   size_t off_f[2][6], off_cb[3], off_kd[6], off_rkd[6], off_be, off_ce, off_bh, off_ch;
   size_t off_psi[2][6][3][2];
-  size_t off_jsrc, off_tw[4], off_ring, off_acc, off_state, off_params, off_tmaps, off_items, off_zero;
+  size_t off_jsrc, off_tw[4], off_ring, off_acc, off_state, off_tmaps, off_items;
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
 };
 
 // Work items of one 3D job: tiles of TY x TZ cells in (y, z), chunks of L
 // planes in x over the updated planes [ib, ie).
-std::vector<SweepItem> sweep_items(const oidt_job_desc *d, int L, int job) {
+std::vector<SweepItem> sweep_items(const oidt_job_desc *d, int L) {
   std::vector<SweepItem> v;
   for (int x0 = d->ib; x0 < d->ie; x0 += L)
     for (int y0 = 0; y0 < d->ny; y0 += TY)
-      for (int z0 = 0; z0 < d->nz; z0 += TZ) v.push_back({job, y0, z0, x0, std::min(x0 + L, d->ie)});
+      for (int z0 = 0; z0 < d->nz; z0 += TZ) v.push_back({y0, z0, x0, std::min(x0 + L, d->ie)});
   return v;
 }
 
@@ -373,12 +337,10 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->off_ring = L.take((size_t)K * 2 * nslot_of(d->mode) * plane * esz);
   pl->off_acc = L.take((size_t)2 * ncomp_of(d->mode) * d->nf * plane * 16);
   pl->off_state = L.take(64);
-  pl->off_zero = pl->off_state + 32;  // a device int 0 (parity base of a single job)
-  pl->off_params = L.take(4 * std::max(sizeof(Params<float>), sizeof(Params<double>)));
   if (variant == kVariantSweep) {
     pl->off_tmaps = L.take(15 * 128);
     pl->L = choose_chunk(d, g_sweep_slots > 0 ? g_sweep_slots : 148 * 3);
-    pl->nitems = (int)sweep_items(d, pl->L, 0).size();
+    pl->nitems = (int)sweep_items(d, pl->L).size();
     pl->off_items = L.take((size_t)pl->nitems * sizeof(SweepItem));
   }
   pl->total = L.off;
@@ -411,20 +373,15 @@ struct Job {
   bool busy = false;
 };
 
-struct BatchPlan {  // cached multi-job composition
+struct BatchPlan {  // cached multi-job composition: one CUDA graph per K-step block
   std::vector<uint64_t> ids;
   std::vector<int> pars;
-  unsigned char *mem = nullptr;
-  Tile *tiles = nullptr;
-  int ntiles = 0;
-  SweepItem *items = nullptr;
-  int nitems = 0;
-  void *pcell = nullptr, *pview = nullptr;
-  int *par0 = nullptr;
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
   int K = 0;
 };
+
+constexpr int kAuxStreams = 16;
 
 }  // namespace
 
@@ -432,6 +389,8 @@ struct oidt_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;  // compute
   cudaStream_t upload = nullptr;  // job creation copies
+  cudaStream_t aux[kAuxStreams] = {};  // branches of multi-job blocks
+  cudaEvent_t fork = nullptr, join[kAuxStreams] = {};
   uint64_t budget = 0, in_use = 0;
   std::map<uint64_t, Job *> jobs;
   uint64_t next_id = 1;
@@ -486,13 +445,13 @@ EncodeTiled encoder() {
   return fn;
 }
 
-// 3D map over a pitched [nx][ny][nzp] array; box [1][TY+2][TZ+8] (z fastest).
+// 3D map over a pitched [nx][ny][nzp] array; box [1][EY+1][EZ+8] (z fastest).
 bool encode_map(CUtensorMap *m, void *base, int esz, int nzp, int ny, int nx) {
   EncodeTiled enc = encoder();
   if (!enc) return false;
   const cuuint64_t dims[3] = {(cuuint64_t)nzp, (cuuint64_t)ny, (cuuint64_t)nx};
   const cuuint64_t strides[2] = {(cuuint64_t)nzp * esz, (cuuint64_t)ny * nzp * esz};
-  const cuuint32_t box[3] = {(cuuint32_t)(TZ + 8), (cuuint32_t)(TY + 2), 1};
+  const cuuint32_t box[3] = {(cuuint32_t)SweepGeom<float, EYB, EZB>::BZ, (cuuint32_t)SweepGeom<float, EYB, EZB>::BY, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   return enc(m, esz == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides,
              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -620,7 +579,6 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
   for (int t = 0; t < 4; ++t)
     CU(ctx, cudaMemcpyAsync(m + pl.off_tw[t], tw[t], (size_t)d.nf * d.nt * 8, cudaMemcpyHostToDevice, st));
   fill_params<T>(J);
-  CU(ctx, cudaMemcpyAsync(m + pl.off_params, views<T>(J), 2 * sizeof(Params<T>), cudaMemcpyHostToDevice, st));
   if (pl.variant == kVariantSweep) {
     std::vector<CUtensorMap> maps(15);
     for (int b = 0; b < 2; ++b)
@@ -631,7 +589,7 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
       if (!encode_map(&maps[12 + c], m + pl.off_cb[c], pl.esz, pl.nzp, d.ny, d.nx))
         return fail(ctx, OIDT_ERR_CUDA, "cuTensorMapEncodeTiled failed (cb map)");
     CU(ctx, cudaMemcpyAsync(m + pl.off_tmaps, maps.data(), 15 * sizeof(CUtensorMap), cudaMemcpyHostToDevice, st));
-    std::vector<SweepItem> it = sweep_items(&d, pl.L, 0);
+    std::vector<SweepItem> it = sweep_items(&d, pl.L);
     CU(ctx, cudaMemcpyAsync(m + pl.off_items, it.data(), it.size() * sizeof(SweepItem), cudaMemcpyHostToDevice, st));
     CU(ctx, cudaStreamSynchronize(st));  // maps and items are host temporaries
   }
@@ -641,21 +599,19 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
   return OIDT_OK;
 }
 
-template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, TY, TZ, ST>(); }
+template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, EYB, EZB, ST>(); }
 
 template <typename T, bool EXACT>
-void launch_sweep(const Params<T> *dparams, const int *dpar0, const SweepItem *items, int nitems, int par, int s,
-                  cudaStream_t st) {
-  k_sweep3d<T, EXACT, TY, TZ, ST><<<nitems, TY * TZ, sweep_smem<T>(), st>>>(dparams, dpar0, items, par, s);
+void launch_sweep(const Params<T> &p, const SweepItem *items, int nitems, int s, cudaStream_t st) {
+  k_sweep3d<T, EXACT, EYB, EZB, ST><<<nitems, EYB * EZB, sweep_smem<T>(), st>>>(p, items, s);
 }
 
 // One time step of one job (s = step offset inside the K block, par = the
 // buffer holding the state at this step).
 template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s, int par, cudaStream_t st) {
   if (J->pl.variant == kVariantSweep) {
-    const Params<T> *dp = reinterpret_cast<const Params<T> *>(J->mem + J->pl.off_params);
-    launch_sweep<T, EXACT>(dp, reinterpret_cast<const int *>(J->mem + J->pl.off_zero),
-                           reinterpret_cast<const SweepItem *>(J->mem + J->pl.off_items), J->pl.nitems, par, s, st);
+    launch_sweep<T, EXACT>(views<T>(J)[par], reinterpret_cast<const SweepItem *>(J->mem + J->pl.off_items),
+                           J->pl.nitems, s, st);
     ctx->launches += 1;
     return;
   }
@@ -729,93 +685,39 @@ int advance(oidt_ctx *ctx, Job *J, int nsteps) {
 }
 
 // ---- multi-job launches ----------------------------------------------------
+// A block of cnt steps for several jobs: each job's launches (its steps, then
+// its DFT fold) go to one of the auxiliary streams, forked from and joined
+// back into the compute stream, so independent jobs run concurrently and the
+// whole block is one CUDA graph when captured.
 void drop_batch(BatchPlan &bp) {
   if (bp.graph) cudaGraphExecDestroy(bp.graph);
   bp.graph = nullptr;
-  if (bp.mem) cudaFree(bp.mem);
-  bp.mem = nullptr;
   bp.ids.clear();
   bp.pars.clear();
 }
 
-template <typename T, bool EXACT>
-int batch_plan(oidt_ctx *ctx, std::vector<Job *> &js) {
-  BatchPlan &bp = ctx->batch;
-  std::vector<uint64_t> ids;
-  std::vector<int> pars;
-  for (Job *j : js) ids.push_back(j->id), pars.push_back(j->parity);
-  if (bp.mem && bp.ids == ids && bp.pars == pars && bp.K == js[0]->pl.K) return OIDT_OK;
-  drop_batch(bp);
-  std::vector<Tile> tiles;
-  std::vector<SweepItem> items;
-  std::vector<Params<T>> pcell, pview;
-  std::vector<int> par0;
+template <typename T, bool EXACT> int batch_block(oidt_ctx *ctx, std::vector<Job *> &js, int cnt, cudaStream_t st) {
+  const int na = std::min<int>(kAuxStreams, (int)js.size());
+  CU(ctx, cudaEventRecord(ctx->fork, st));
+  for (int a = 0; a < na; ++a) CU(ctx, cudaStreamWaitEvent(ctx->aux[a], ctx->fork, 0));
   for (int b = 0; b < (int)js.size(); ++b) {
     Job *J = js[b];
-    const oidt_job_desc &d = J->d;
-    pcell.push_back(cells<T>(J)[J->parity]);
-    pview.push_back(views<T>(J)[0]);
-    pview.push_back(views<T>(J)[1]);
-    par0.push_back(J->parity);
-    if (J->pl.variant == kVariantSweep) {
-      std::vector<SweepItem> it = sweep_items(&d, J->pl.L, b);
-      items.insert(items.end(), it.begin(), it.end());
-    } else if (d.mode == OIDT_MODE_YEE3D) {
-      for (int i = 0; i < d.nx; ++i)
-        for (int j0 = 0; j0 < d.ny; j0 += kBlock3Y)
-          for (int k0 = 0; k0 < d.nz; k0 += kBlock3Z) tiles.push_back({b, i, j0, k0});
-    } else {
-      for (int i = 0; i < d.nx; ++i)
-        for (int j0 = 0; j0 < d.ny; j0 += kBlock2) tiles.push_back({b, i, j0, 0});
-    }
+    cudaStream_t sb = ctx->aux[b % na];
+    const int flip = steps_flip(J);
+    for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, J->parity ^ (flip & s), sb);
+    launch_fold<T, EXACT>(ctx, J, cnt, sb);
   }
-  Layout L;
-  const size_t o_t = L.take(tiles.size() * sizeof(Tile) + 16), o_i = L.take(items.size() * sizeof(SweepItem) + 16);
-  const size_t o_c = L.take(pcell.size() * sizeof(Params<T>)), o_v = L.take(pview.size() * sizeof(Params<T>));
-  const size_t o_p = L.take(par0.size() * sizeof(int));
-  CU(ctx, cudaMalloc(&bp.mem, L.off));
-  CU(ctx, cudaMemcpy(bp.mem + o_t, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
-  CU(ctx, cudaMemcpy(bp.mem + o_i, items.data(), items.size() * sizeof(SweepItem), cudaMemcpyHostToDevice));
-  CU(ctx, cudaMemcpy(bp.mem + o_c, pcell.data(), pcell.size() * sizeof(Params<T>), cudaMemcpyHostToDevice));
-  CU(ctx, cudaMemcpy(bp.mem + o_v, pview.data(), pview.size() * sizeof(Params<T>), cudaMemcpyHostToDevice));
-  CU(ctx, cudaMemcpy(bp.mem + o_p, par0.data(), par0.size() * sizeof(int), cudaMemcpyHostToDevice));
-  bp.tiles = reinterpret_cast<Tile *>(bp.mem + o_t);
-  bp.items = reinterpret_cast<SweepItem *>(bp.mem + o_i);
-  bp.pcell = bp.mem + o_c;
-  bp.pview = bp.mem + o_v;
-  bp.par0 = reinterpret_cast<int *>(bp.mem + o_p);
-  bp.ntiles = (int)tiles.size();
-  bp.nitems = (int)items.size();
-  bp.ids = ids;
-  bp.pars = pars;
-  bp.K = js[0]->pl.K;
+  for (int a = 0; a < na; ++a) {
+    CU(ctx, cudaEventRecord(ctx->join[a], ctx->aux[a]));
+    CU(ctx, cudaStreamWaitEvent(st, ctx->join[a], 0));
+  }
   return OIDT_OK;
-}
-
-// s-th step of a block for every job of the plan: sweep jobs launch-step
-// parity s & 1 relative to their parity at plan time; per-cell jobs run in
-// place on their current buffer.
-template <typename T, bool EXACT> void batch_block(oidt_ctx *ctx, std::vector<Job *> &js, int cnt, cudaStream_t st) {
-  BatchPlan &bp = ctx->batch;
-  const Params<T> *dc = reinterpret_cast<const Params<T> *>(bp.pcell);
-  const Params<T> *dv = reinterpret_cast<const Params<T> *>(bp.pview);
-  for (int s = 0; s < cnt; ++s) {
-    if (bp.nitems) {
-      launch_sweep<T, EXACT>(dv, bp.par0, bp.items, bp.nitems, s & 1, s, st);
-      ctx->launches += 1;
-    }
-    if (bp.ntiles) {
-      k_batch<T, EXACT, true><<<bp.ntiles, 128, 0, st>>>(dc, bp.tiles, s);
-      k_batch<T, EXACT, false><<<bp.ntiles, 128, 0, st>>>(dc, bp.tiles, s);
-      ctx->launches += 2;
-    }
-  }
-  for (Job *j : js) launch_fold<T, EXACT>(ctx, j, cnt, st);
 }
 
 template <typename T, bool EXACT>
 int batch_t(oidt_ctx *ctx, std::vector<Job *> &js, int nsteps) {
   cudaStream_t st = ctx->stream;
+  BatchPlan &bp = ctx->batch;
   const int K = js[0]->pl.K;
   for (Job *j : js) {
     if (j->pl.K != K) return fail(ctx, OIDT_ERR_INVALID, "batched jobs must share ring_steps");
@@ -823,17 +725,26 @@ int batch_t(oidt_ctx *ctx, std::vector<Job *> &js, int nsteps) {
   }
   int left = nsteps;
   while (left > 0) {
-    int rc = batch_plan<T, EXACT>(ctx, js);
-    if (rc) return rc;
-    BatchPlan &bp = ctx->batch;
+    std::vector<uint64_t> ids;
+    std::vector<int> pars;
+    for (Job *j : js) ids.push_back(j->id), pars.push_back(j->parity);
+    if (bp.ids != ids || bp.pars != pars || bp.K != K) {
+      drop_batch(bp);
+      bp.ids = ids;
+      bp.pars = pars;
+      bp.K = K;
+    }
     const int cnt = std::min(K, left);
+    int rc = OIDT_OK;
     if (cnt == K && (K & 1) == 0) {
       if (!bp.graph) {
         cudaGraph_t g;
         const long long before = ctx->launches;
         CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        batch_block<T, EXACT>(ctx, js, K, st);
-        CU(ctx, cudaStreamEndCapture(st, &g));
+        rc = batch_block<T, EXACT>(ctx, js, K, st);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (rc) return rc;
+        CU(ctx, ce);
         bp.graph_launches = ctx->launches - before;
         ctx->launches = before;
         CU(ctx, cudaGraphInstantiate(&bp.graph, g, 0));
@@ -842,7 +753,8 @@ int batch_t(oidt_ctx *ctx, std::vector<Job *> &js, int nsteps) {
       CU(ctx, cudaGraphLaunch(bp.graph, st));
       ctx->launches += bp.graph_launches;
     } else {
-      batch_block<T, EXACT>(ctx, js, cnt, st);
+      rc = batch_block<T, EXACT>(ctx, js, cnt, st);
+      if (rc) return rc;
       if (cnt & 1)  // sweep jobs end this block on the other buffer
         for (Job *j : js) j->parity ^= steps_flip(j);
     }
@@ -948,14 +860,15 @@ void destroy_job(oidt_ctx *ctx, Job *J) {
 }
 
 int set_sweep_attrs() {
-  cudaFuncSetAttribute(k_sweep3d<float, false, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<float>());
-  cudaFuncSetAttribute(k_sweep3d<float, true, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<float>());
-  cudaFuncSetAttribute(k_sweep3d<double, false, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<double>());
-  cudaFuncSetAttribute(k_sweep3d<double, true, TY, TZ, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<double>());
+  cudaFuncSetAttribute(k_sweep3d<float, false, EYB, EZB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<float>());
+  // (each launch passes its job's parameters by value: about 1 KB of kernel parameter space)
+  cudaFuncSetAttribute(k_sweep3d<float, true, EYB, EZB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<float>());
+  cudaFuncSetAttribute(k_sweep3d<double, false, EYB, EZB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<double>());
+  cudaFuncSetAttribute(k_sweep3d<double, true, EYB, EZB, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sweep_smem<double>());
   int per_sm = 0, sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep3d<float, false, TY, TZ, ST>, TY * TZ, sweep_smem<float>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep3d<float, false, EYB, EZB, ST>, EYB * EZB, sweep_smem<float>());
   return std::max(1, per_sm) * std::max(1, sms);
 }
 
@@ -980,6 +893,11 @@ int32_t oidt_create(int32_t device, uint64_t hbm_budget, oidt_ctx **out) {
     delete ctx;
     return OIDT_ERR_CUDA;
   }
+  for (int a = 0; a < kAuxStreams; ++a) {
+    cudaStreamCreateWithFlags(&ctx->aux[a], cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&ctx->join[a], cudaEventDisableTiming);
+  }
+  cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
   g_sweep_slots = set_sweep_attrs();
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
@@ -998,6 +916,12 @@ int32_t oidt_destroy(oidt_ctx *ctx) {
     ctx->jobs.clear();
     drop_batch(ctx->batch);
     cudaStreamSynchronize(ctx->stream);
+    for (int a = 0; a < kAuxStreams; ++a) {
+      cudaStreamSynchronize(ctx->aux[a]);
+      cudaStreamDestroy(ctx->aux[a]);
+      cudaEventDestroy(ctx->join[a]);
+    }
+    cudaEventDestroy(ctx->fork);
     cudaStreamDestroy(ctx->stream);
     cudaStreamDestroy(ctx->upload);
   }

@@ -2,22 +2,29 @@
 // updated in a single sweep over x-planes, each plane of a CTA's tile staged
 // in shared memory by TMA (cp.async.bulk.tensor, no multicast).
 //
-// Work item = (job, y0, z0, x0, x1): the CTA owns cells y in [y0, y0+TY),
-// z in [z0, z0+TZ) of planes x in [x0, x1).  Per plane i it needs, from the
-// old buffers, H(i) and H(i+1) over a one-cell halo and E(i), dt/eps(i) over
-// the low halo; it computes the new E over the tile plus its low halo (the
-// halo cells recompute what the neighbouring tile computes, so no exchange
-// is needed), then the new H of its own cells, and writes new E and H to the
-// other buffer (ping-pong).  Every field word is read once and written once
-// per step from HBM (60 B per cell in FP32); halo re-reads hit L2.
+// Work item = (y0, z0, x0, x1) of one job.  The CTA has EY x EZ threads; thread
+// (ey, ez) is cell y = y0 - 1 + ey, z = z0 - 1 + ez for every plane of the
+// item.  Cells with ey, ez >= 1 are owned (the tile is (EY-1) x (EZ-1)); row
+// ey = 0 and column ez = 0 are the low halo, whose new E the tile recomputes
+// because its H update needs E(j-1) and E(k-1) -- so tiles never exchange
+// data within a step.  Per plane i the CTA needs H(i) and H(i+1) over the
+// box rows y0-1 .. y0+EY-1 and columns z0-1 .. z0+EZ-1, plus E(i) and dt/eps(i);
+// it writes new E and H of its owned cells to the other buffer (ping-pong).
+// Every field word is read once and written once per step from HBM (60 B per
+// cell in FP32); halo re-reads hit L2.
 //
-// Shared memory per CTA: S stages x 9 boxes [TY+2][TZ+8] (fields + dt/eps of
-// one plane; z starts 4 cells before z0 so the TMA x-coordinate stays 16-byte
-// aligned) + two planes of new E over the tile + low halo.
+// A thread keeps its cell's old H and new E in registers from the E half to
+// the H half, and its new Ey, Ez for the next plane (the x-differences of the
+// H update); in-plane E neighbours come from a double-buffered shared tile.
+// Range tests, CPML slab positions and kappa*dx factors that depend on (j, k)
+// are computed once per work item, those that depend on i once per plane.
+// Operand order equals kernels.cuh (y3_e_compute / y3_h_compute), which
+// follows the reference kernels, so OIDT_ARITH_EXACT results match bit for bit.
 //
-// Waits on the TMA mbarriers are bounded: after kWaitCycles clock cycles the
-// CTA records an error in state[1], stops issuing work, gives the copies still
-// in flight the same bounded time to land, and returns.
+// TMA boxes start at z = floor4(z0 - 1) (16-byte aligned x-coordinate) and
+// y = y0 - 1; out-of-range rows/columns read as zero.  Waits on the TMA
+// mbarriers are bounded (kWaitCycles): on expiry the CTA records an error in
+// state[1], stops issuing, waits the same bound for copies in flight, returns.
 #pragma once
 #include <cuda.h>
 
@@ -26,11 +33,13 @@
 namespace oidt {
 
 struct SweepItem {
-  int job, y0, z0, x0, x1;
+  int y0, z0, x0, x1;
 };
 
-constexpr int kSweepTY = 8, kSweepTZ = 32, kSweepStages = 3;
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz: bounded TMA wait
+// E-box of the CTA: EY x EZ threads, owned tile (EY-1) x (EZ-1).
+constexpr int kSweepEY = 8, kSweepEZ = 32, kSweepStages = 3;
+constexpr int kSweepTY = kSweepEY - 1, kSweepTZ = kSweepEZ - 1;  // owned tile
+constexpr long long kWaitCycles = 4000000000LL;                  // ~2 s at 1.9 GHz
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -61,76 +70,102 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int c0,
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Shared-memory accessor for one cell of the tile.
-template <typename T, int TY, int TZ> struct BoxAcc3 {
-  static constexpr int BY = TY + 2, BZ = TZ + 8, BOX = BY * BZ, EY_ = TY + 1, EZ_ = TZ + 1, EBOX = EY_ * EZ_;
-  // box stride in shared memory: each TMA destination starts 128-byte aligned
-  static constexpr int BOXS = (int)(((BOX * sizeof(T) + 127) / 128) * 128 / sizeof(T));
-  const T *cur;   // stage of plane i: 9 boxes
-  const T *nxt;   // stage of plane i+1
-  const T *enew;  // new E of plane i: 3 x [EY_][EZ_]
-  const T *eprv;  // new E of plane i-1
-  int bo;         // box offset of the cell: (y-(y0-1))*BZ + (z-(z0-4))
-  int eo;         // E-box offset of the cell: (y-(y0-1))*EZ_ + (z-(z0-1))
-  __device__ __forceinline__ T h(int f, int di, int dj, int dk) const {
-    return (di ? nxt : cur)[f * BOXS + bo + dj * BZ + dk];
-  }
-  __device__ __forceinline__ T e(int f, int di, int dj, int dk) const {
-    return di ? eprv[f * EBOX + eo] : enew[f * EBOX + eo + dj * EZ_ + dk];
-  }
-  __device__ __forceinline__ T eold(int f) const { return cur[f * BOXS + bo]; }
-  __device__ __forceinline__ T hold(int f) const { return cur[f * BOXS + bo]; }
-  __device__ __forceinline__ T cb(int a) const { return cur[(6 + a) * BOXS + bo]; }
+template <typename T, int EY, int EZ> struct SweepGeom {
+  static constexpr int BY = EY + 1;         // box rows: y0-1 .. y0+EY-1
+  static constexpr int BZ = EZ + 8;         // box cols from floor4(z0-1): covers z0-1 .. z0+EZ-1 (+3 slack)
+  static constexpr int BOX = BY * BZ;
+  static constexpr int BOXS = (int)(((BOX * sizeof(T) + 127) / 128) * 128 / sizeof(T));  // 128-B aligned boxes
+  static constexpr int NT = EY * EZ;
 };
 
-template <typename T, int TY, int TZ, int S>
+template <typename T, int EY, int EZ, int S>
 constexpr size_t sweep_smem_bytes() {
-  return (size_t)S * 9 * BoxAcc3<T, TY, TZ>::BOXS * sizeof(T) + 2 * 3 * (TY + 1) * (TZ + 1) * sizeof(T) +
-         sizeof(Params<T>) + 8 * S + 3 * 128;
+  using G = SweepGeom<T, EY, EZ>;
+  return (size_t)S * 9 * G::BOXS * sizeof(T) + 2 * 3 * G::NT * sizeof(T) + 8 * S + 2 * 128;
 }
 
-// params[job] holds the parity-0 and parity-1 views of each job (which
-// buffer is old and which is new); `par` selects one for this step.
-template <typename T, bool EXACT, int TY, int TZ, int S>
-__global__ void __launch_bounds__(TY *TZ) k_sweep3d(const Params<T> *__restrict__ params, const int *__restrict__ par0,
-                                                    const SweepItem *__restrict__ items, int par, int s) {
-  using Acc = BoxAcc3<T, TY, TZ>;
-  constexpr int NT = TY * TZ, BOX = Acc::BOX, BOXS = Acc::BOXS, BZ = Acc::BZ, EZ_ = Acc::EZ_, EBOX = Acc::EBOX;
+// Packed CPML slab position: q (coefficient index) | d << 12 | side << 24, or -1.
+__device__ __forceinline__ int slab_code_e(int c, int b, int e, int P) {
+  int d, side;
+  const int q = e_slab(c, b, e, P, d, side);
+  return q < 0 ? -1 : (q | (d << 12) | (side << 24));
+}
+__device__ __forceinline__ int slab_code_h(int c, int b, int e, int P) {
+  int d, side;
+  const int q = h_slab(c, b, e, P, d, side);
+  return q < 0 ? -1 : (q | (d << 12) | (side << 24));
+}
+__device__ __forceinline__ int sq(int code) { return code & 0xfff; }
+__device__ __forceinline__ int sd(int code) { return (code >> 12) & 0xfff; }
+__device__ __forceinline__ int ss(int code) { return code >> 24; }
+
+// `p` is the job's view for this step (which buffer is old and which is
+// new), passed in the kernel's parameter space so every field is a constant
+// operand; `items` is the job's tile table.
+template <typename T, bool EXACT, int EY, int EZ, int S>
+__global__ void __launch_bounds__(EY *EZ) k_sweep3d(const __grid_constant__ Params<T> p,
+                                                    const SweepItem *__restrict__ items, int s) {
+  using G = SweepGeom<T, EY, EZ>;
+  using A = Ar<T, EXACT>;
+  constexpr int NT = G::NT, BZ = G::BZ, BOX = G::BOX, BOXS = G::BOXS;
   constexpr unsigned STAGE_BYTES = 9u * BOX * sizeof(T);
-  static_assert(sizeof(Params<T>) % 8 == 0, "Params must be a whole number of 8-byte words");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
   T *stage = reinterpret_cast<T *>(smem);
-  T *sE = stage + S * 9 * BOXS;
-  unsigned long long *sp = reinterpret_cast<unsigned long long *>(
-      (reinterpret_cast<uintptr_t>(sE + 2 * 3 * EBOX) + 127) & ~uintptr_t(127));
-  unsigned long long *bar = sp + sizeof(Params<T>) / 8;
-  __shared__ int s_abort;
+  T *sE = stage + S * 9 * BOXS;  // [2][3][NT]
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(
+      (reinterpret_cast<uintptr_t>(sE + 2 * 3 * NT) + 127) & ~uintptr_t(127));
+  __shared__ int s_abort, s_issued, s_failed;
 
   const SweepItem it = items[blockIdx.x];
   const int tid = threadIdx.x;
-  {
-    const unsigned long long *src =
-        reinterpret_cast<const unsigned long long *>(params + 2 * it.job + ((par ^ par0[it.job]) & 1));
-    for (int w = tid; w < (int)(sizeof(Params<T>) / 8); w += NT) sp[w] = src[w];
-  }
-  __syncthreads();  // the parameter copy must be complete before any thread reads it
-  const Params<T> &p = *reinterpret_cast<const Params<T> *>(sp);
+  const int ey = tid / EZ, ez = tid % EZ;
   const int y0 = it.y0, z0 = it.z0, x0 = it.x0, x1 = it.x1;
-  const int xs = x0 - 1;          // first plane loaded (E of x0-1 feeds H of x0)
+  const int zb = (z0 - 1) & ~3;  // box column origin (floor to a multiple of 4)
+  const int zoff = (z0 - 1) - zb;
+  const int xs = x0 - 1;            // first plane loaded (E of x0-1 feeds H of x0)
   const int nplanes = x1 - xs + 1;  // planes xs .. x1
   const int n = p.state[0] + s;
+  const int y = y0 - 1 + ey, z = z0 - 1 + ez;
+  const bool ingrid = y >= 0 && y < p.ny && z >= 0 && z < p.nz;
+  const bool own = ingrid && ey >= 1 && ez >= 1;
+  const int bo = ey * BZ + ez + zoff;  // this cell in a box
+  const int P = p.P;
+
+  // ---- per-item (j, k) classification --------------------------------------
+  const bool jin_c = y >= p.jb && y < p.je, jin_o = y > p.jb && y < p.je;   // [jb,je) and (jb,je)
+  const bool kin_c = z >= p.kb && z < p.ke, kin_o = z > p.kb && z < p.ke;
+  const bool ex_jk = ingrid && jin_c && kin_c;   // Ex: j [jb,je), k [kb,ke)
+  const bool ey_jk = ingrid && jin_o && kin_c;   // Ey: j (jb,je), k [kb,ke)
+  const bool ez_jk = ingrid && jin_c && kin_o;   // Ez: j [jb,je), k (kb,ke)
+  const bool hx_jk = own && jin_o && kin_o;      // Hx: j (jb,je), k (kb,ke)
+  const bool hy_jk = own && jin_c && kin_o;      // Hy: j [jb,je), k (kb,ke)
+  const bool hz_jk = own && jin_o && kin_c;      // Hz: j (jb,je), k [kb,ke)
+  const int ye_code = ingrid ? slab_code_e(y, p.jb, p.je, P) : -1;
+  const int ze_code = ingrid ? slab_code_e(z, p.kb, p.ke, P) : -1;
+  const int yh_code = own ? slab_code_h(y, p.jb, p.je, P) : -1;
+  const int zh_code = own ? slab_code_h(z, p.kb, p.ke, P) : -1;
+  const int yc = ingrid ? y : 0, zc = ingrid ? z : 0;
+  const T kye = EXACT ? p.kd[1][yc] : T(0), rkye = p.rkd[1][yc];
+  const T kze = EXACT ? p.kd[2][zc] : T(0), rkze = p.rkd[2][zc];
+  const T kyh = EXACT ? p.kd[4][yc] : T(0), rkyh = p.rkd[4][yc];
+  const T kzh = EXACT ? p.kd[5][zc] : T(0), rkzh = p.rkd[5][zc];
+  const bool src_jk = p.src_field >= 0 && y >= p.slo[1] && y < p.shi[1] && z >= p.slo[2] && z < p.shi[2];
+  const bool src_jk1 = p.src_field == HY && y >= p.slo[1] && y < p.shi[1] && z + 1 >= p.slo[2] && z + 1 < p.shi[2];
+  const bool capt = own && (z == p.port_pos[0] || z == p.port_pos[1] || z == p.port_pos[0] + 1 ||
+                            z == p.port_pos[1] + 1);
+  const long long g_jk = (long long)y * p.nzp + z;  // cell offset inside a plane
+
   const unsigned char *tmf = static_cast<const unsigned char *>(p.tmap_f);
   const unsigned char *tmc = static_cast<const unsigned char *>(p.tmap_cb);
-
   auto issue = [&](int u) {  // load plane xs+u into stage u % S
     T *dst = stage + (u % S) * 9 * BOXS;
     unsigned long long *b = bar + (u % S);
     fence_proxy_async();
     mbar_expect_tx(b, STAGE_BYTES);
     const int xi = xs + u;
-    for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * BOXS, tmf + f * 128, z0 - 4, y0 - 1, xi, b);
-    for (int a = 0; a < 3; ++a) tma_load_3d(dst + (6 + a) * BOXS, tmc + a * 128, z0 - 4, y0 - 1, xi, b);
+    for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * BOXS, tmf + f * 128, zb, y0 - 1, xi, b);
+    for (int a = 0; a < 3; ++a) tma_load_3d(dst + (6 + a) * BOXS, tmc + a * 128, zb, y0 - 1, xi, b);
   };
   auto wait = [&](int u) -> bool {
     unsigned long long *b = bar + (u % S);
@@ -141,77 +176,226 @@ __global__ void __launch_bounds__(TY *TZ) k_sweep3d(const Params<T> *__restrict_
     }
     return true;
   };
-  __shared__ int s_issued, s_failed;
 
   if (tid == 0) {
     s_abort = 0;
+    s_failed = 0x7fffffff;
     for (int k = 0; k < S; ++k) mbar_init(bar + k, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   if (tid == 0) {
-    s_issued = 0;
-    s_failed = 0x7fffffff;
-    for (int u = 0; u < S && u < nplanes; ++u) issue(u), s_issued = u + 1;
+    int u = 0;
+    for (; u < S - 1 && u < nplanes; ++u) issue(u);
+    s_issued = u;
   }
-  __syncthreads();
-
   bool ok = wait(0);
   if (!ok) atomicMin(&s_failed, 0);
-  for (int u = 0; u + 1 < nplanes; ++u) {  // plane i = xs + u, needs stage u and u+1
+  T ey_prev = T(0), ez_prev = T(0);  // new Ey, Ez of this cell at the previous plane
+
+  for (int u = 0; u + 1 < nplanes; ++u) {
     const int i = xs + u;
     if (ok && !(ok = wait(u + 1))) atomicMin(&s_failed, u + 1);
-    if (!ok) s_abort = 1;
-    __syncthreads();
-    if (s_abort) break;
     const T *cur = stage + (u % S) * 9 * BOXS;
     const T *nxt = stage + ((u + 1) % S) * 9 * BOXS;
-    T *enew = sE + (u & 1) * 3 * EBOX;
-    const T *eprv = sE + ((u + 1) & 1) * 3 * EBOX;
-    // ---- new E over the tile and its low halo -----------------------------
-    for (int e = tid; e < EBOX; e += NT) {
-      const int ey = e / EZ_, ez = e % EZ_;
-      const int y = y0 - 1 + ey, z = z0 - 1 + ez;
-      T ev[3] = {T(0), T(0), T(0)};
-      if (y >= 0 && y < p.ny && z >= 0 && z < p.nz) {
-        Acc a{cur, nxt, enew, eprv, ey * BZ + ez + 3, e};
-        const bool own = ey >= 1 && ez >= 1 && i >= x0;
-        y3_e_compute<T, EXACT>(p, a, i, y, z, n, own, ev);
-      }
-      enew[e] = ev[0];
-      enew[EBOX + e] = ev[1];
-      enew[2 * EBOX + e] = ev[2];
-    }
-    __syncthreads();
-    // ---- new H of the tile's cells; store E and H ---------------------------
-    if (i >= x0) {
-      for (int c = tid; c < TY * TZ; c += NT) {
-        const int ty = c / TZ, tz = c % TZ;
-        const int y = y0 + ty, z = z0 + tz;
-        if (y >= p.ny || z >= p.nz) continue;
-        const int eo = (ty + 1) * EZ_ + tz + 1;
-        Acc a{cur, nxt, enew, eprv, (ty + 1) * BZ + tz + 4, eo};
-        T hv[3];
-        const int mh = y3_h_compute<T, EXACT>(p, a, i, y, z, n, hv);
-        const long long g = ((long long)i * p.ny + y) * p.nzp + z;
-        const T ev[3] = {enew[eo], enew[EBOX + eo], enew[2 * EBOX + eo]};
-        p.fn[EX][g] = ev[0];
-        p.fn[EY][g] = ev[1];
-        p.fn[EZ][g] = ev[2];
-        p.fn[HX][g] = hv[0];
-        p.fn[HY][g] = hv[1];
-        p.fn[HZ][g] = hv[2];
-        if (z == p.port_pos[0] || z == p.port_pos[1] || z == p.port_pos[0] + 1 || z == p.port_pos[1] + 1) {
-          // capture only components the step updated (the others stay zero)
-          const int me = (i > p.ib && i < p.ie && y >= p.jb && y < p.je && z >= p.kb && z < p.ke ? 1 : 0) |
-                         (i >= p.ib && i < p.ie && y > p.jb && y < p.je && z >= p.kb && z < p.ke ? 2 : 0);
-          y3_capture_e(p, s, i, y, z, me, ev);
-          y3_capture_h(p, s, i, y, z, mh, hv);
+    T *enew = sE + (u & 1) * 3 * NT;
+    // ---- per-plane values ----------------------------------------------------
+    const bool i_c = i >= p.ib && i < p.ie, i_o = i > p.ib && i < p.ie;
+    const int xe_code = slab_code_e(i, p.ib, p.ie, P);
+    const int xh_code = slab_code_h(i, p.ib, p.ie, P);
+    const T kxe = EXACT ? p.kd[0][i] : T(0), rkxe = p.rkd[0][i];
+    const T kxh = EXACT ? p.kd[3][i] : T(0), rkxh = p.rkd[3][i];
+    const bool src_i = i >= p.slo[0] && i < p.shi[0];
+    const bool src_i1 = i + 1 >= p.slo[0] && i + 1 < p.shi[0];
+    const T Jn = p.src_field >= 0 ? p.jsrc[n] : T(0);
+    // ---- new E of this cell (all threads of the E box) ------------------------
+    T hx0 = T(0), hy0 = T(0), hz0 = T(0), e0 = T(0), e1 = T(0), e2 = T(0);
+    int me = 0;
+    if (ok && ingrid) {
+      hx0 = cur[HX * BOXS + bo];
+      hy0 = cur[HY * BOXS + bo];
+      hz0 = cur[HZ * BOXS + bo];
+      e0 = cur[EX * BOXS + bo];
+      e1 = cur[EY * BOXS + bo];
+      e2 = cur[EZ * BOXS + bo];
+      const bool wpsi = own && i >= x0;  // this CTA owns the cell's new psi
+      if (i_o && ex_jk) {  // Ex                                     fdtd_funcs.py:43-50, 113-136
+        const T cb = cur[(6 + 0) * BOXS + bo];
+        const T dhz = A::sub(cur[HZ * BOXS + bo + BZ], hz0);
+        const T hy1 = cur[HY * BOXS + bo + 1];
+        const T dhy = A::sub(hy1, hy0);
+        T e = A::add(e0, A::mul(cb, A::sub(A::div(dhz, kye, rkye), A::div(dhy, kze, rkze))));
+        if (ye_code >= 0) {
+          const int q = sq(ye_code);
+          const long long o = psi_idx3(AY, i, sd(ye_code), z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.be[q], p.psi[EX][AY][ss(ye_code)][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
+          if (wpsi) p.psin[EX][AY][ss(ye_code)][o] = v;
+          e = A::add(e, A::mul(cb, v));
         }
+        if (ze_code >= 0) {
+          T h1 = hy1, h0 = hy0;
+          if (p.src_field == HY) {
+            if (src_i && src_jk1) h1 = A::sub(h1, Jn);
+            if (src_i && src_jk) h0 = A::sub(h0, Jn);
+          }
+          const int q = sq(ze_code);
+          const long long o = psi_idx3(AZ, i, y, sd(ze_code), p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.be[q], p.psi[EX][AZ][ss(ze_code)][o]),
+                             A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
+          if (wpsi) p.psin[EX][AZ][ss(ze_code)][o] = v;
+          e = A::sub(e, A::mul(cb, v));
+        }
+        e0 = e;
+        me |= 1;
+      }
+      if (i_c && ey_jk) {  // Ey                                     :53-60, 104-110, 139-162
+        const T cb = cur[(6 + 1) * BOXS + bo];
+        const T dhx = A::sub(cur[HX * BOXS + bo + 1], hx0);
+        const T dhz = A::sub(nxt[HZ * BOXS + bo], hz0);
+        T e = A::add(e1, A::mul(cb, A::sub(A::div(dhx, kze, rkze), A::div(dhz, kxe, rkxe))));
+        if (p.src_field == EY && src_i && src_jk) e = A::sub(e, Jn);
+        if (xe_code >= 0) {
+          const int q = sq(xe_code);
+          const long long o = psi_idx3(AX, sd(xe_code), y, z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.be[q], p.psi[EY][AX][ss(xe_code)][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
+          if (wpsi) p.psin[EY][AX][ss(xe_code)][o] = v;
+          e = A::sub(e, A::mul(cb, v));
+        }
+        if (ze_code >= 0) {
+          const int q = sq(ze_code);
+          const long long o = psi_idx3(AZ, i, y, sd(ze_code), p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.be[q], p.psi[EY][AZ][ss(ze_code)][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
+          if (wpsi) p.psin[EY][AZ][ss(ze_code)][o] = v;
+          e = A::add(e, A::mul(cb, v));
+        }
+        e1 = e;
+        me |= 2;
+      }
+      if (i_c && ez_jk) {  // Ez                                     :63-70, 165-188
+        const T cb = cur[(6 + 2) * BOXS + bo];
+        const T hy1 = nxt[HY * BOXS + bo];
+        const T dhy = A::sub(hy1, hy0);
+        const T dhx = A::sub(cur[HX * BOXS + bo + BZ], hx0);
+        T e = A::add(e2, A::mul(cb, A::sub(A::div(dhy, kxe, rkxe), A::div(dhx, kye, rkye))));
+        if (xe_code >= 0) {
+          T h1 = hy1, h0 = hy0;
+          if (p.src_field == HY) {
+            if (src_i1 && src_jk) h1 = A::sub(h1, Jn);
+            if (src_i && src_jk) h0 = A::sub(h0, Jn);
+          }
+          const int q = sq(xe_code);
+          const long long o = psi_idx3(AX, sd(xe_code), y, z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.be[q], p.psi[EZ][AX][ss(xe_code)][o]),
+                             A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
+          if (wpsi) p.psin[EZ][AX][ss(xe_code)][o] = v;
+          e = A::add(e, A::mul(cb, v));
+        }
+        if (ye_code >= 0) {
+          const int q = sq(ye_code);
+          const long long o = psi_idx3(AY, i, sd(ye_code), z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.be[q], p.psi[EZ][AY][ss(ye_code)][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
+          if (wpsi) p.psin[EZ][AY][ss(ye_code)][o] = v;
+          e = A::sub(e, A::mul(cb, v));
+        }
+        e2 = e;
+        me |= 4;
       }
     }
-    __syncthreads();
-    if (tid == 0 && u + S < nplanes) issue(u + S), s_issued = u + S + 1;  // stage u is free now
+    enew[tid] = e0;
+    enew[NT + tid] = e1;
+    enew[2 * NT + tid] = e2;
+    if (!ok) s_abort = 1;
+    __syncthreads();  // new E of the tile visible; stage (u-1) % S no longer read
+    if (s_abort) break;
+    if (tid == 0 && u + S - 1 < nplanes) {
+      issue(u + S - 1);  // into stage (u-1) % S
+      s_issued = u + S;
+    }
+    // ---- new H of owned cells; store E and H ------------------------------------
+    if (own && i >= x0) {
+      T h0v = hx0, h1v = hy0, h2v = hz0;
+      int mh = 0;
+      const T db = p.db;
+      if (i_c && hx_jk) {  // Hx                                     :73-80, 191-214
+        const T dey = A::sub(e1, enew[NT + tid - 1]);
+        const T dez = A::sub(e2, enew[2 * NT + tid - EZ]);
+        T h = A::add(h0v, A::mul(db, A::sub(A::div(dey, kzh, rkzh), A::div(dez, kyh, rkyh))));
+        if (yh_code >= 0) {
+          const int q = sq(yh_code);
+          T *ps = p.psi[HX][AY][ss(yh_code)] + psi_idx3(AY, i, sd(yh_code), z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
+          *ps = v;
+          h = A::sub(h, A::mul(db, v));
+        }
+        if (zh_code >= 0) {
+          const int q = sq(zh_code);
+          T *ps = p.psi[HX][AZ][ss(zh_code)] + psi_idx3(AZ, i, y, sd(zh_code), p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
+          *ps = v;
+          h = A::add(h, A::mul(db, v));
+        }
+        h0v = h;
+        mh |= 1;
+      }
+      if (i_o && hy_jk) {  // Hy                                     :83-90, 217-240
+        const T dez = A::sub(e2, ez_prev);
+        const T dex = A::sub(e0, enew[tid - 1]);
+        T h = h1v;
+        if (p.src_field == HY && src_i && src_jk) h = A::sub(h, Jn);  // source precedes update_hy
+        h = A::add(h, A::mul(db, A::sub(A::div(dez, kxh, rkxh), A::div(dex, kzh, rkzh))));
+        if (xh_code >= 0) {
+          const int q = sq(xh_code);
+          T *ps = p.psi[HY][AX][ss(xh_code)] + psi_idx3(AX, sd(xh_code), y, z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
+          *ps = v;
+          h = A::add(h, A::mul(db, v));
+        }
+        if (zh_code >= 0) {
+          const int q = sq(zh_code);
+          T *ps = p.psi[HY][AZ][ss(zh_code)] + psi_idx3(AZ, i, y, sd(zh_code), p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
+          *ps = v;
+          h = A::sub(h, A::mul(db, v));
+        }
+        h1v = h;
+        mh |= 2;
+      }
+      if (i_o && hz_jk) {  // Hz                                     :93-100, 243-266
+        const T dex = A::sub(e0, enew[tid - EZ]);
+        const T dey = A::sub(e1, ey_prev);
+        T h = A::add(h2v, A::mul(db, A::sub(A::div(dex, kyh, rkyh), A::div(dey, kxh, rkxh))));
+        if (xh_code >= 0) {
+          const int q = sq(xh_code);
+          T *ps = p.psi[HZ][AX][ss(xh_code)] + psi_idx3(AX, sd(xh_code), y, z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
+          *ps = v;
+          h = A::sub(h, A::mul(db, v));
+        }
+        if (yh_code >= 0) {
+          const int q = sq(yh_code);
+          T *ps = p.psi[HZ][AY][ss(yh_code)] + psi_idx3(AY, i, sd(yh_code), z, p.nx, p.ny, p.nz, P);
+          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
+          *ps = v;
+          h = A::add(h, A::mul(db, v));
+        }
+        h2v = h;
+        mh |= 4;
+      }
+      const long long g = (long long)i * p.ny * p.nzp + g_jk;
+      p.fn[EX][g] = e0;
+      p.fn[EY][g] = e1;
+      p.fn[EZ][g] = e2;
+      p.fn[HX][g] = h0v;
+      p.fn[HY][g] = h1v;
+      p.fn[HZ][g] = h2v;
+      if (capt) {
+        const T ev[3] = {e0, e1, e2}, hv[3] = {h0v, h1v, h2v};
+        y3_capture_e(p, s, i, y, z, me, ev);
+        y3_capture_h(p, s, i, y, z, mh, hv);
+      }
+    }
+    ey_prev = e1;
+    ez_prev = e2;
   }
   if (s_abort && tid == 0) {
     atomicExch(p.state + 1, 1);  // reported to the host by oidt_job_sync
