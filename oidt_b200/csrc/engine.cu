@@ -134,15 +134,20 @@ __device__ __forceinline__ double coloc(const FoldParams<T> &fp, int port, int c
   }
 }
 
+// One block: 128 window cells x kFoldF frequencies of one (port, component).
+// The block's twiddles for up to kFoldChunk steps are staged in shared memory
+// (every thread uses the same values), accumulators stay in registers.
+constexpr int kFoldChunk = 32;
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
   using A = Ar<double, EXACT>;
+  __shared__ double2 tw[kFoldChunk][kFoldF];
   const int wj = fp.whi1 - fp.wlo1;
   const int wi = fp.mode == OIDT_MODE_YEE3D ? fp.whi0 - fp.wlo0 : 1;
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= wi * wj) return;
-  const int i = fp.mode == OIDT_MODE_YEE3D ? fp.wlo0 + w / wj : 0;
-  const int j = fp.wlo1 + w % wj;
+  const bool active = w < wi * wj;
+  const int i = fp.mode == OIDT_MODE_YEE3D ? fp.wlo0 + (active ? w / wj : 0) : 0;
+  const int j = fp.wlo1 + (active ? w % wj : 0);
   const int port = blockIdx.z / fp.ncomp, comp = blockIdx.z % fp.ncomp;
   const bool hcomp = fp.mode == OIDT_MODE_YEE3D ? comp >= 2 : comp == 1;
   const double *cs = fp.tw[hcomp ? 2 : 0], *sn = fp.tw[hcomp ? 3 : 1];
@@ -152,24 +157,38 @@ __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
   double2 *acc = fp.acc + (((long long)port * fp.ncomp + comp) * fp.nf + f0) * fp.plane + cell;
   double re[kFoldF], im[kFoldF];
 #pragma unroll
-  for (int f = 0; f < kFoldF; ++f)
-    if (f < nfc) { double2 a = acc[f * fp.plane]; re[f] = a.x; im[f] = a.y; }
+  for (int f = 0; f < kFoldF; ++f) {
+    re[f] = 0.0;
+    im[f] = 0.0;
+    if (active && f < nfc) { double2 a = acc[f * fp.plane]; re[f] = a.x; im[f] = a.y; }
+  }
   const int n0 = fp.state[0];
-  for (int s = 0; s < count; ++s) {
-    const double x = coloc<T, EXACT>(fp, port, comp, s, i, j);
-    const long long n = n0 + s;
+  for (int s0 = 0; s0 < count; s0 += kFoldChunk) {
+    const int sc = min(kFoldChunk, count - s0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < sc * kFoldF; t += blockDim.x) {
+      const int ss = t / kFoldF, f = t % kFoldF;
+      const long long idx = (long long)(f0 + f) * fp.nt + n0 + s0 + ss;
+      tw[ss][f] = f < nfc ? make_double2(__ldg(cs + idx), __ldg(sn + idx)) : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (active) {
+      for (int ss = 0; ss < sc; ++ss) {
+        const double x = coloc<T, EXACT>(fp, port, comp, s0 + ss, i, j);
 #pragma unroll
-    for (int f = 0; f < kFoldF; ++f) {
-      if (f < nfc) {
-        const long long t = (long long)(f0 + f) * fp.nt + n;
-        re[f] = A::add(re[f], A::mul(x, __ldg(cs + t)));
-        im[f] = A::sub(im[f], A::mul(x, __ldg(sn + t)));
+        for (int f = 0; f < kFoldF; ++f) {
+          const double2 t = tw[ss][f];
+          re[f] = A::add(re[f], A::mul(x, t.x));
+          im[f] = A::sub(im[f], A::mul(x, t.y));
+        }
       }
     }
   }
+  if (active) {
 #pragma unroll
-  for (int f = 0; f < kFoldF; ++f)
-    if (f < nfc) acc[f * fp.plane] = make_double2(re[f], im[f]);
+    for (int f = 0; f < kFoldF; ++f)
+      if (f < nfc) acc[f * fp.plane] = make_double2(re[f], im[f]);
+  }
 }
 
 __global__ void k_bump(int *state, int count) {

@@ -2,13 +2,13 @@
 // updated in a single sweep over x-planes, each plane of a CTA's tile staged
 // in shared memory by TMA (cp.async.bulk.tensor, no multicast).
 //
-// Work item = (y0, z0, x0, x1) of one job.  The CTA has EY x EZ threads; thread
+// Work item = (y0, z0, x0, x1) of one job.  The CTA has TBY x TBZ threads; thread
 // (ey, ez) is cell y = y0 - 1 + ey, z = z0 - 1 + ez for every plane of the
-// item.  Cells with ey, ez >= 1 are owned (the tile is (EY-1) x (EZ-1)); row
+// item.  Cells with ey, ez >= 1 are owned (the tile is (TBY-1) x (TBZ-1)); row
 // ey = 0 and column ez = 0 are the low halo, whose new E the tile recomputes
 // because its H update needs E(j-1) and E(k-1) -- so tiles never exchange
 // data within a step.  Per plane i the CTA needs H(i) and H(i+1) over the
-// box rows y0-1 .. y0+EY-1 and columns z0-1 .. z0+EZ-1, plus E(i) and dt/eps(i);
+// box rows y0-1 .. y0+TBY-1 and columns z0-1 .. z0+TBZ-1, plus E(i) and dt/eps(i);
 // it writes new E and H of its owned cells to the other buffer (ping-pong).
 // Every field word is read once and written once per step from HBM (60 B per
 // cell in FP32); halo re-reads hit L2.
@@ -36,7 +36,7 @@ struct SweepItem {
   int y0, z0, x0, x1;
 };
 
-// E-box of the CTA: EY x EZ threads, owned tile (EY-1) x (EZ-1).
+// E-box of the CTA: TBY x TBZ threads, owned tile (TBY-1) x (TBZ-1).
 constexpr int kSweepEY = 8, kSweepEZ = 32, kSweepStages = 3;
 constexpr int kSweepTY = kSweepEY - 1, kSweepTZ = kSweepEZ - 1;  // owned tile
 constexpr long long kWaitCycles = 4000000000LL;                  // ~2 s at 1.9 GHz
@@ -70,17 +70,17 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int c0,
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-template <typename T, int EY, int EZ> struct SweepGeom {
-  static constexpr int BY = EY + 1;         // box rows: y0-1 .. y0+EY-1
-  static constexpr int BZ = EZ + 8;         // box cols from floor4(z0-1): covers z0-1 .. z0+EZ-1 (+3 slack)
+template <typename T, int TBY, int TBZ> struct SweepGeom {
+  static constexpr int BY = TBY + 1;         // box rows: y0-1 .. y0+TBY-1
+  static constexpr int BZ = TBZ + 8;         // box cols from floor4(z0-1): covers z0-1 .. z0+TBZ-1 (+3 slack)
   static constexpr int BOX = BY * BZ;
   static constexpr int BOXS = (int)(((BOX * sizeof(T) + 127) / 128) * 128 / sizeof(T));  // 128-B aligned boxes
-  static constexpr int NT = EY * EZ;
+  static constexpr int NT = TBY * TBZ;
 };
 
-template <typename T, int EY, int EZ, int S>
+template <typename T, int TBY, int TBZ, int S>
 constexpr size_t sweep_smem_bytes() {
-  using G = SweepGeom<T, EY, EZ>;
+  using G = SweepGeom<T, TBY, TBZ>;
   return (size_t)S * 9 * G::BOXS * sizeof(T) + 2 * 3 * G::NT * sizeof(T) + 8 * S + 2 * 128;
 }
 
@@ -102,10 +102,10 @@ __device__ __forceinline__ int ss(int code) { return code >> 24; }
 // `p` is the job's view for this step (which buffer is old and which is
 // new), passed in the kernel's parameter space so every field is a constant
 // operand; `items` is the job's tile table.
-template <typename T, bool EXACT, int EY, int EZ, int S>
-__global__ void __launch_bounds__(EY *EZ) k_sweep3d(const __grid_constant__ Params<T> p,
+template <typename T, bool EXACT, int TBY, int TBZ, int S>
+__global__ void __launch_bounds__(TBY *TBZ) k_sweep3d(const __grid_constant__ Params<T> p,
                                                     const SweepItem *__restrict__ items, int s) {
-  using G = SweepGeom<T, EY, EZ>;
+  using G = SweepGeom<T, TBY, TBZ>;
   using A = Ar<T, EXACT>;
   constexpr int NT = G::NT, BZ = G::BZ, BOX = G::BOX, BOXS = G::BOXS;
   constexpr unsigned STAGE_BYTES = 9u * BOX * sizeof(T);
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(EY *EZ) k_sweep3d(const __grid_constant__ Para
 
   const SweepItem it = items[blockIdx.x];
   const int tid = threadIdx.x;
-  const int ey = tid / EZ, ez = tid % EZ;
+  const int ey = tid / TBZ, ez = tid % TBZ;
   const int y0 = it.y0, z0 = it.z0, x0 = it.x0, x1 = it.x1;
   const int zb = (z0 - 1) & ~3;  // box column origin (floor to a multiple of 4)
   const int zoff = (z0 - 1) - zb;
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(EY *EZ) k_sweep3d(const __grid_constant__ Para
       const T db = p.db;
       if (i_c && hx_jk) {  // Hx                                     :73-80, 191-214
         const T dey = A::sub(e1, enew[NT + tid - 1]);
-        const T dez = A::sub(e2, enew[2 * NT + tid - EZ]);
+        const T dez = A::sub(e2, enew[2 * NT + tid - TBZ]);
         T h = A::add(h0v, A::mul(db, A::sub(A::div(dey, kzh, rkzh), A::div(dez, kyh, rkyh))));
         if (yh_code >= 0) {
           const int q = sq(yh_code);
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(EY *EZ) k_sweep3d(const __grid_constant__ Para
         mh |= 2;
       }
       if (i_o && hz_jk) {  // Hz                                     :93-100, 243-266
-        const T dex = A::sub(e0, enew[tid - EZ]);
+        const T dex = A::sub(e0, enew[tid - TBZ]);
         const T dey = A::sub(e1, ey_prev);
         T h = A::add(h2v, A::mul(db, A::sub(A::div(dex, kyh, rkyh), A::div(dey, kxh, rkxh))));
         if (xh_code >= 0) {
