@@ -163,7 +163,6 @@ def pinned_spec(spec, prec):
         t = torch.empty(a.shape, dtype=torch.float32 if dt == np.float32 else torch.float64, pin_memory=True)
         out = t.numpy()
         out[...] = a
-        out._keep = t if False else None  # noqa: the tensor is kept below
         keep.append(t)
         return out
 

@@ -248,19 +248,56 @@ struct JobPlan {
   int K, esz, nzp, nbuf, variant, L, nitems;
 };
 
+// Flags of the work item whose E box starts at (y0 - 1, z0 - 1) (rows
+// y0-1 .. y0+EYB-2, columns z0-1 .. z0+EZB-2).
+int item_flags(const oidt_job_desc *d, int y0, int z0) {
+  const int ylo = y0 - 1, yhi = y0 + EYB - 2, zlo = z0 - 1, zhi = z0 + EZB - 2, P = d->num_cpml;
+  auto meets = [](int lo, int hi, int a, int b) { return a <= b && lo <= b && a <= hi; };  // [lo,hi] and [a,b] intersect
+  int f = 0;
+  if (ylo <= d->jb || yhi >= d->je || zlo <= d->kb || zhi >= d->ke) f |= kItemEdge;
+  if (meets(ylo, yhi, d->jb, d->jb + P - 1) || meets(ylo, yhi, d->je - P, d->je - 1)) f |= kItemYSlab;
+  if (meets(zlo, zhi, d->kb, d->kb + P - 1) || meets(zlo, zhi, d->ke - P, d->ke - 1)) f |= kItemZSlab;
+  if (d->src_field >= 0 && meets(ylo, yhi, d->src_lo[1], d->src_hi[1] - 1) &&
+      meets(zlo, zhi, d->src_lo[2] - 1, d->src_hi[2] - 1))  // z - 1: the Hy source also enters at k + 1
+    f |= kItemSrc;
+  for (int q = 0; q < 2; ++q)
+    if (meets(z0, zhi, d->port_pos[q], d->port_pos[q] + 1)) f |= kItemPort;
+  return f;
+}
+
+// Relative cost of a tile's plane: general planes run the range tests and
+// the CPML updates of their slabs.
+double tile_weight(int flags) {
+  double w = 1.0;
+  if (flags) w += 0.6;
+  if (flags & (kItemYSlab | kItemZSlab)) w += 0.8;
+  return w;
+}
+
 // Work items of one 3D job: tiles of TY x TZ cells in (y, z), chunks of L
-// planes in x over the updated planes [ib, ie).
+// planes in x over the updated planes [ib, ie).  Tiles are ordered by
+// decreasing weight (the block scheduler then fills the last wave with cheap
+// tiles), the chunks of one tile are adjacent (their shared halo planes are
+// read while still in L2).
 std::vector<SweepItem> sweep_items(const oidt_job_desc *d, int L) {
+  struct Tile { int y0, z0, f; double w; };
+  std::vector<Tile> tiles;
+  for (int y0 = 0; y0 < d->ny; y0 += TY)
+    for (int z0 = 0; z0 < d->nz; z0 += TZ) {
+      const int f = item_flags(d, y0, z0);
+      tiles.push_back({y0, z0, f, tile_weight(f)});
+    }
+  std::stable_sort(tiles.begin(), tiles.end(), [](const Tile &a, const Tile &b) { return a.w > b.w; });
   std::vector<SweepItem> v;
-  for (int x0 = d->ib; x0 < d->ie; x0 += L)
-    for (int y0 = 0; y0 < d->ny; y0 += TY)
-      for (int z0 = 0; z0 < d->nz; z0 += TZ) v.push_back({y0, z0, x0, std::min(x0 + L, d->ie)});
+  for (const Tile &t : tiles)
+    for (int x0 = d->ib; x0 < d->ie; x0 += L) v.push_back({t.y0, t.z0, x0, std::min(x0 + L, d->ie), t.f, 0, 0, 0});
   return v;
 }
 
-// March depth: the chunk length that best fills whole waves of resident CTAs
-// (item cost ~ L + 2 planes, the extra planes being the E and H halos along
-// x).  OIDT_SWEEP_L overrides.  `slots` = SMs x resident CTAs per SM.
+// March depth: the chunk length L minimising the estimated makespan of one
+// step, (total plane iterations) / (resident CTAs) + (one item's length);
+// an item of L planes iterates L + 1 times (the E halo plane x0 - 1).
+// OIDT_SWEEP_L overrides.  `slots` = SMs x resident CTAs per SM.
 int choose_chunk(const oidt_job_desc *d, int slots) {
   if (const char *e = getenv("OIDT_SWEEP_L")) {
     int v = atoi(e);
@@ -272,9 +309,7 @@ int choose_chunk(const oidt_job_desc *d, int slots) {
   int bestL = planes;
   for (int L = 4; L <= planes; ++L) {
     const long long chunks = (planes + L - 1) / L;
-    const long long items = tiles * chunks;
-    const long long waves = (items + slots - 1) / slots;
-    const double cost = (double)waves * (L + 2);  // critical path in plane-iterations
+    const double cost = (double)tiles * (planes + chunks) / slots + (L + 1);
     if (cost < best - 1e-9) { best = cost; bestL = L; }
   }
   return bestL;
@@ -622,7 +657,7 @@ template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, EYB, EZB,
 
 template <typename T, bool EXACT>
 void launch_sweep(const Params<T> &p, const SweepItem *items, int nitems, int s, cudaStream_t st) {
-  k_sweep3d<T, EXACT, EYB, EZB, ST><<<nitems, EYB * EZB, sweep_smem<T>(), st>>>(p, items, s);
+  k_sweep3d<T, EXACT, EYB, EZB, ST><<<nitems, SweepGeom<T, EYB, EZB>::THREADS, sweep_smem<T>(), st>>>(p, items, s);
 }
 
 // One time step of one job (s = step offset inside the K block, par = the
@@ -887,7 +922,7 @@ int set_sweep_attrs() {
   int per_sm = 0, sms = 0, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep3d<float, false, EYB, EZB, ST>, EYB * EZB, sweep_smem<float>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep3d<float, false, EYB, EZB, ST>, SweepGeom<float, EYB, EZB>::THREADS, sweep_smem<float>());
   return std::max(1, per_sm) * std::max(1, sms);
 }
 

@@ -28,12 +28,28 @@
 #pragma once
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace oidt {
 
+// Work item flags, CTA-uniform, set on the host per item.  Every plane runs
+// the three curl updates of each component unconditionally; the source, the
+// CPML terms, the DFT capture and the per-cell range masks are each behind a
+// branch on these flags (or on the plane index), so a plane of an unflagged
+// item outside both x CPML slabs runs no per-cell test at all.
+enum : int {
+  kItemEdge = 1,   // some E-box cell lies outside (jb, je) x (kb, ke) (or outside the grid)
+  kItemYSlab = 2,  // some E-box cell lies in a y CPML slab
+  kItemZSlab = 4,  // some E-box cell lies in a z CPML slab
+  kItemSrc = 8,    // the source box meets the item's (y, z) columns
+  kItemPort = 16,  // an owned column lies on a port plane (DFT capture)
+};
+
 struct SweepItem {
   int y0, z0, x0, x1;
+  int flags, pad0, pad1, pad2;
 };
 
 // E-box of the CTA: TBY x TBZ threads, owned tile (TBY-1) x (TBZ-1).
@@ -75,7 +91,8 @@ template <typename T, int TBY, int TBZ> struct SweepGeom {
   static constexpr int BZ = TBZ + 8;         // box cols from floor4(z0-1): covers z0-1 .. z0+TBZ-1 (+3 slack)
   static constexpr int BOX = BY * BZ;
   static constexpr int BOXS = (int)(((BOX * sizeof(T) + 127) / 128) * 128 / sizeof(T));  // 128-B aligned boxes
-  static constexpr int NT = TBY * TBZ;
+  static constexpr int NT = TBY * TBZ;                      // cells of the E box
+  static constexpr int THREADS = NT;                        // one thread per cell
 };
 
 template <typename T, int TBY, int TBZ, int S>
@@ -100,24 +117,37 @@ __device__ __forceinline__ int sd(int code) { return (code >> 12) & 0xfff; }
 __device__ __forceinline__ int ss(int code) { return code >> 24; }
 
 // `p` is the job's view for this step (which buffer is old and which is
-// new), passed in the kernel's parameter space so every field is a constant
-// operand; `items` is the job's tile table.
+// new), passed in the kernel's parameter space; `items` is the job's tile
+// table.
+//
+// Pipeline: S stages of plane boxes.  Plane u+1 must be resident when plane u
+// is processed (the E update reads H(i+1)); the stage of plane u is refilled
+// with plane u+S right after the barrier that ends plane u's E half, so loads
+// run S-1 planes ahead.
+//
+// Items without flags (every E-box cell strictly inside the update ranges
+// and outside the y and z CPML slabs, no source, no port) run a specialised
+// march whose only decisions are per plane (boundary planes, x CPML planes);
+// flagged items run the general march with per-cell range masks.
 template <typename T, bool EXACT, int TBY, int TBZ, int S>
-__global__ void __launch_bounds__(TBY *TBZ) k_sweep3d(const __grid_constant__ Params<T> p,
-                                                    const SweepItem *__restrict__ items, int s) {
+__global__ void __launch_bounds__(TBY *TBZ, sizeof(T) == 4 ? 4 : 2)
+    k_sweep3d(const __grid_constant__ Params<T> p, const SweepItem *__restrict__ items, int s) {
+  static_assert(S >= 3, "the stage refilled after plane u must differ from those of planes u+1, u+2");
   using G = SweepGeom<T, TBY, TBZ>;
   using A = Ar<T, EXACT>;
-  constexpr int NT = G::NT, BZ = G::BZ, BOX = G::BOX, BOXS = G::BOXS;
+  constexpr int NT = G::NT, BZ = G::BZ, BOX = G::BOX, BOXS = G::BOXS, SB = 9 * BOXS;
   constexpr unsigned STAGE_BYTES = 9u * BOX * sizeof(T);
+  // Shared memory is addressed as offsets from the __shared__ array itself
+  // (no integer round trip), so every access compiles to a shared load/store.
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  unsigned char *smem = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  T *stage = reinterpret_cast<T *>(smem);
-  T *sE = stage + S * 9 * BOXS;  // [2][3][NT]
-  unsigned long long *bar = reinterpret_cast<unsigned long long *>(
-      (reinterpret_cast<uintptr_t>(sE + 2 * 3 * NT) + 127) & ~uintptr_t(127));
-  __shared__ int s_abort, s_issued, s_failed;
+  const unsigned pad = (128u - (smem_u32(smem_raw) & 127u)) & 127u;
+  T *const stage = reinterpret_cast<T *>(smem_raw + pad);  // [S][9][BOXS]
+  T *const sE = stage + S * SB;                              // [2][3][NT]
+  unsigned long long *const bar = reinterpret_cast<unsigned long long *>(sE + 2 * 3 * NT);
+  __shared__ int s_abort[2], s_issued, s_failed;  // s_abort[u & 1]: plane u's verdict
 
   const SweepItem it = items[blockIdx.x];
+  const int fl = it.flags;
   const int tid = threadIdx.x;
   const int ey = tid / TBZ, ez = tid % TBZ;
   const int y0 = it.y0, z0 = it.z0, x0 = it.x0, x1 = it.x1;
@@ -130,36 +160,24 @@ __global__ void __launch_bounds__(TBY *TBZ) k_sweep3d(const __grid_constant__ Pa
   const bool ingrid = y >= 0 && y < p.ny && z >= 0 && z < p.nz;
   const bool own = ingrid && ey >= 1 && ez >= 1;
   const int bo = ey * BZ + ez + zoff;  // this cell in a box
-  const int P = p.P;
-
-  // ---- per-item (j, k) classification --------------------------------------
-  const bool jin_c = y >= p.jb && y < p.je, jin_o = y > p.jb && y < p.je;   // [jb,je) and (jb,je)
-  const bool kin_c = z >= p.kb && z < p.ke, kin_o = z > p.kb && z < p.ke;
-  const bool ex_jk = ingrid && jin_c && kin_c;   // Ex: j [jb,je), k [kb,ke)
-  const bool ey_jk = ingrid && jin_o && kin_c;   // Ey: j (jb,je), k [kb,ke)
-  const bool ez_jk = ingrid && jin_c && kin_o;   // Ez: j [jb,je), k (kb,ke)
-  const bool hx_jk = own && jin_o && kin_o;      // Hx: j (jb,je), k (kb,ke)
-  const bool hy_jk = own && jin_c && kin_o;      // Hy: j [jb,je), k (kb,ke)
-  const bool hz_jk = own && jin_o && kin_c;      // Hz: j (jb,je), k [kb,ke)
-  const int ye_code = ingrid ? slab_code_e(y, p.jb, p.je, P) : -1;
-  const int ze_code = ingrid ? slab_code_e(z, p.kb, p.ke, P) : -1;
-  const int yh_code = own ? slab_code_h(y, p.jb, p.je, P) : -1;
-  const int zh_code = own ? slab_code_h(z, p.kb, p.ke, P) : -1;
+  const int P = p.P, ny = p.ny, nz = p.nz, ib = p.ib, ie = p.ie;
+  const long long plane_f = (long long)p.ny * p.nzp;  // field elements per x-plane
+  const long long g_jk = (long long)y * p.nzp + z;   // cell offset inside a plane
+  const long long plane_ax = (long long)ny * nz;     // AX psi elements per slab layer
+  const int off_ax = y * nz + z;                      // AX psi offset inside a slab layer
+  T *const fEX = p.fn[EX], *const fEY = p.fn[EY], *const fEZ = p.fn[EZ];
+  T *const fHX = p.fn[HX], *const fHY = p.fn[HY], *const fHZ = p.fn[HZ];
+  const T db = p.db, dx = p.dx, rdx = p.rdx;
   const int yc = ingrid ? y : 0, zc = ingrid ? z : 0;
   const T kye = EXACT ? p.kd[1][yc] : T(0), rkye = p.rkd[1][yc];
   const T kze = EXACT ? p.kd[2][zc] : T(0), rkze = p.rkd[2][zc];
   const T kyh = EXACT ? p.kd[4][yc] : T(0), rkyh = p.rkd[4][yc];
   const T kzh = EXACT ? p.kd[5][zc] : T(0), rkzh = p.rkd[5][zc];
-  const bool src_jk = p.src_field >= 0 && y >= p.slo[1] && y < p.shi[1] && z >= p.slo[2] && z < p.shi[2];
-  const bool src_jk1 = p.src_field == HY && y >= p.slo[1] && y < p.shi[1] && z + 1 >= p.slo[2] && z + 1 < p.shi[2];
-  const bool capt = own && (z == p.port_pos[0] || z == p.port_pos[1] || z == p.port_pos[0] + 1 ||
-                            z == p.port_pos[1] + 1);
-  const long long g_jk = (long long)y * p.nzp + z;  // cell offset inside a plane
 
   const unsigned char *tmf = static_cast<const unsigned char *>(p.tmap_f);
   const unsigned char *tmc = static_cast<const unsigned char *>(p.tmap_cb);
   auto issue = [&](int u) {  // load plane xs+u into stage u % S
-    T *dst = stage + (u % S) * 9 * BOXS;
+    T *dst = stage + (u % S) * SB;
     unsigned long long *b = bar + (u % S);
     fence_proxy_async();
     mbar_expect_tx(b, STAGE_BYTES);
@@ -167,18 +185,18 @@ __global__ void __launch_bounds__(TBY *TBZ) k_sweep3d(const __grid_constant__ Pa
     for (int f = 0; f < 6; ++f) tma_load_3d(dst + f * BOXS, tmf + f * 128, zb, y0 - 1, xi, b);
     for (int a = 0; a < 3; ++a) tma_load_3d(dst + (6 + a) * BOXS, tmc + a * 128, zb, y0 - 1, xi, b);
   };
-  auto wait = [&](int u) -> bool {
-    unsigned long long *b = bar + (u % S);
-    const unsigned ph = (unsigned)((u / S) & 1);
+  // plane u lives in stage u % S and completes that stage's phase u / S
+  auto wait = [&](int k, unsigned parity) -> bool {
+    if (mbar_try_wait(bar + k, parity)) return true;
     const long long t0 = clock64();
-    while (!mbar_try_wait(b, ph)) {
+    while (!mbar_try_wait(bar + k, parity)) {
       if (clock64() - t0 > kWaitCycles) return false;
     }
     return true;
   };
 
   if (tid == 0) {
-    s_abort = 0;
+    s_abort[0] = s_abort[1] = 0;
     s_failed = 0x7fffffff;
     for (int k = 0; k < S; ++k) mbar_init(bar + k, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -186,221 +204,312 @@ __global__ void __launch_bounds__(TBY *TBZ) k_sweep3d(const __grid_constant__ Pa
   __syncthreads();
   if (tid == 0) {
     int u = 0;
-    for (; u < S - 1 && u < nplanes; ++u) issue(u);
+    for (; u < S && u < nplanes; ++u) issue(u);
     s_issued = u;
   }
-  bool ok = wait(0);
+  bool ok = wait(0, 0);
   if (!ok) atomicMin(&s_failed, 0);
-  T ey_prev = T(0), ez_prev = T(0);  // new Ey, Ez of this cell at the previous plane
+  bool aborted = false;
 
-  for (int u = 0; u + 1 < nplanes; ++u) {
-    const int i = xs + u;
-    if (ok && !(ok = wait(u + 1))) atomicMin(&s_failed, u + 1);
-    const T *cur = stage + (u % S) * 9 * BOXS;
-    const T *nxt = stage + ((u + 1) % S) * 9 * BOXS;
-    T *enew = sE + (u & 1) * 3 * NT;
-    // ---- per-plane values ----------------------------------------------------
-    const bool i_c = i >= p.ib && i < p.ie, i_o = i > p.ib && i < p.ie;
-    const int xe_code = slab_code_e(i, p.ib, p.ie, P);
-    const int xh_code = slab_code_h(i, p.ib, p.ie, P);
-    const T kxe = EXACT ? p.kd[0][i] : T(0), rkxe = p.rkd[0][i];
-    const T kxh = EXACT ? p.kd[3][i] : T(0), rkxh = p.rkd[3][i];
-    const bool src_i = i >= p.slo[0] && i < p.shi[0];
-    const bool src_i1 = i + 1 >= p.slo[0] && i + 1 < p.shi[0];
-    const T Jn = p.src_field >= 0 ? p.jsrc[n] : T(0);
-    // ---- new E of this cell (all threads of the E box) ------------------------
-    T hx0 = T(0), hy0 = T(0), hz0 = T(0), e0 = T(0), e1 = T(0), e2 = T(0);
-    int me = 0;
-    if (ok && ingrid) {
-      hx0 = cur[HX * BOXS + bo];
-      hy0 = cur[HY * BOXS + bo];
-      hz0 = cur[HZ * BOXS + bo];
-      e0 = cur[EX * BOXS + bo];
-      e1 = cur[EY * BOXS + bo];
-      e2 = cur[EZ * BOXS + bo];
+  auto march = [&](auto clean_tag) {
+    constexpr bool CLEAN = decltype(clean_tag)::value;
+    // ---- per-cell (j, k) classification (general march only) -----------------
+    const bool jin_c = y >= p.jb && y < p.je, jin_o = y > p.jb && y < p.je;  // [jb,je) and (jb,je)
+    const bool kin_c = z >= p.kb && z < p.ke, kin_o = z > p.kb && z < p.ke;  // [kb,ke) and (kb,ke)
+    const bool ex_jk = CLEAN || (ingrid && jin_c && kin_c);  // Ex: j [jb,je), k [kb,ke)
+    const bool ey_jk = CLEAN || (ingrid && jin_o && kin_c);  // Ey: j (jb,je), k [kb,ke)
+    const bool ez_jk = CLEAN || (ingrid && jin_c && kin_o);  // Ez: j [jb,je), k (kb,ke)
+    const bool hx_jk = CLEAN || (own && jin_o && kin_o);     // Hx: j (jb,je), k (kb,ke)
+    const bool hy_jk = CLEAN || (own && jin_c && kin_o);     // Hy: j [jb,je), k (kb,ke)
+    const bool hz_jk = CLEAN || (own && jin_o && kin_c);     // Hz: j (jb,je), k [kb,ke)
+    const int ye_code = !CLEAN && (fl & kItemYSlab) && ingrid ? slab_code_e(y, p.jb, p.je, P) : -1;
+    const int ze_code = !CLEAN && (fl & kItemZSlab) && ingrid ? slab_code_e(z, p.kb, p.ke, P) : -1;
+    const int yh_code = !CLEAN && (fl & kItemYSlab) && own ? slab_code_h(y, p.jb, p.je, P) : -1;
+    const int zh_code = !CLEAN && (fl & kItemZSlab) && own ? slab_code_h(z, p.kb, p.ke, P) : -1;
+    const bool slab_yz = !CLEAN && (fl & (kItemYSlab | kItemZSlab)) != 0;
+    const bool src_p = !CLEAN && (fl & kItemSrc) != 0;
+    const bool src_jk = src_p && y >= p.slo[1] && y < p.shi[1] && z >= p.slo[2] && z < p.shi[2];
+    const bool src_jk1 =
+        src_p && p.src_field == HY && y >= p.slo[1] && y < p.shi[1] && z + 1 >= p.slo[2] && z + 1 < p.shi[2];
+    const bool capt = !CLEAN && (fl & kItemPort) && own &&
+                      (z == p.port_pos[0] || z == p.port_pos[1] || z == p.port_pos[0] + 1 || z == p.port_pos[1] + 1);
+    const T Jn = src_p ? p.jsrc[n] : T(0);
+    // psi offsets, split into a per-plane base and a per-cell part:
+    // AY slabs [i][d][z] -> i*P*nz + (d*nz + z); AZ slabs [i][y][d] -> i*ny*P + (y*P + d)
+    const int o_ay_e = ye_code >= 0 ? sd(ye_code) * nz + z : 0, o_az_e = ze_code >= 0 ? y * P + sd(ze_code) : 0;
+    const int o_ay_h = yh_code >= 0 ? sd(yh_code) * nz + z : 0, o_az_h = zh_code >= 0 ? y * P + sd(zh_code) : 0;
+
+    T kxe_n = EXACT ? p.kd[0][xs] : T(0), rkxe_n = p.rkd[0][xs];
+    T kxh_n = EXACT ? p.kd[3][xs] : T(0), rkxh_n = p.rkd[3][xs];
+    T ey_prev = T(0), ez_prev = T(0);  // new Ey, Ez of this cell at the previous plane
+    int sc = 0, sn = 1 % S;            // stages of planes u and u+1
+    unsigned pn = (1 / S) & 1;         // phase parity of plane u+1
+
+    for (int u = 0; u + 1 < nplanes; ++u) {
+      const int i = xs + u;
+      if (ok && !(ok = wait(sn, pn))) atomicMin(&s_failed, u + 1);
+      const T *const cur = stage + sc * SB;
+      const T *const nxt = stage + sn * SB;
+      T *const enew = sE + (u & 1) * 3 * NT;
+      // ---- per-plane values (uniform) ------------------------------------------
+      const bool i_c = i >= ib && i < ie, i_o = i > ib && i < ie;
+      const int xe_code = slab_code_e(i, ib, ie, P);
+      const int xh_code = slab_code_h(i, ib, ie, P);
+      const bool edge_p = !CLEAN && ((fl & kItemEdge) || !i_o);  // per-cell range masks needed
+      const T kxe = kxe_n, rkxe = rkxe_n, kxh = kxh_n, rkxh = rkxh_n;
+      if (u + 2 < nplanes) {
+        if (EXACT) { kxe_n = p.kd[0][i + 1]; kxh_n = p.kd[3][i + 1]; }
+        rkxe_n = p.rkd[0][i + 1];
+        rkxh_n = p.rkd[3][i + 1];
+      }
+      const bool src_i = src_p && i >= p.slo[0] && i < p.shi[0];
+      const bool src_i1 = src_p && i + 1 >= p.slo[0] && i + 1 < p.shi[0];
+      const long long b_ay = (long long)i * P * nz, b_az = (long long)i * ny * P;
+      // ---- new E of this cell (all cells of the E box) --------------------------
+      // fdtd_funcs.py:43-70 (curl), :104-110 (source), :113-188 (CPML), in that order
+      const T hx0 = cur[HX * BOXS + bo], hy0 = cur[HY * BOXS + bo], hz0 = cur[HZ * BOXS + bo];
+      T e0 = cur[EX * BOXS + bo], e1 = cur[EY * BOXS + bo], e2 = cur[EZ * BOXS + bo];
+      const T cb0 = cur[6 * BOXS + bo], cb1 = cur[7 * BOXS + bo], cb2 = cur[8 * BOXS + bo];
+      const T hy_z1 = cur[HY * BOXS + bo + 1], hy_x1 = nxt[HY * BOXS + bo];
+      const T dhz_y = A::sub(cur[HZ * BOXS + bo + BZ], hz0);
+      const T dhy_z = A::sub(hy_z1, hy0);
+      const T dhx_z = A::sub(cur[HX * BOXS + bo + 1], hx0);
+      const T dhz_x = A::sub(nxt[HZ * BOXS + bo], hz0);
+      const T dhy_x = A::sub(hy_x1, hy0);
+      const T dhx_y = A::sub(cur[HX * BOXS + bo + BZ], hx0);
+      T nex = A::add(e0, A::mul(cb0, A::sub(A::div(dhz_y, kye, rkye), A::div(dhy_z, kze, rkze))));
+      T ney = A::add(e1, A::mul(cb1, A::sub(A::div(dhx_z, kze, rkze), A::div(dhz_x, kxe, rkxe))));
+      T nez = A::add(e2, A::mul(cb2, A::sub(A::div(dhy_x, kxe, rkxe), A::div(dhx_y, kye, rkye))));
+      const bool mex = i_o && ex_jk, mey = i_c && ey_jk, mez = i_c && ez_jk;  // components updated here
       const bool wpsi = own && i >= x0;  // this CTA owns the cell's new psi
-      if (i_o && ex_jk) {  // Ex                                     fdtd_funcs.py:43-50, 113-136
-        const T cb = cur[(6 + 0) * BOXS + bo];
-        const T dhz = A::sub(cur[HZ * BOXS + bo + BZ], hz0);
-        const T hy1 = cur[HY * BOXS + bo + 1];
-        const T dhy = A::sub(hy1, hy0);
-        T e = A::add(e0, A::mul(cb, A::sub(A::div(dhz, kye, rkye), A::div(dhy, kze, rkze))));
-        if (ye_code >= 0) {
-          const int q = sq(ye_code);
-          const long long o = psi_idx3(AY, i, sd(ye_code), z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.be[q], p.psi[EX][AY][ss(ye_code)][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
-          if (wpsi) p.psin[EX][AY][ss(ye_code)][o] = v;
-          e = A::add(e, A::mul(cb, v));
-        }
-        if (ze_code >= 0) {
-          T h1 = hy1, h0 = hy0;
-          if (p.src_field == HY) {
-            if (src_i && src_jk1) h1 = A::sub(h1, Jn);
-            if (src_i && src_jk) h0 = A::sub(h0, Jn);
+      if (src_i && p.src_field == EY && src_jk) ney = A::sub(ney, Jn);
+      if (CLEAN) {
+        if (xe_code >= 0 && i_c) {  // update_pml_ey_xinc, update_pml_ez_xinc
+          const int q = sq(xe_code), sd_ = ss(xe_code);
+          const long long o = (long long)sd(xe_code) * plane_ax + off_ax;
+          const T vy = A::add(A::mul(p.be[q], __ldg(p.psi[EY][AX][sd_] + o)), A::div(A::mul(p.ce[q], dhz_x), dx, rdx));
+          const T vz = A::add(A::mul(p.be[q], __ldg(p.psi[EZ][AX][sd_] + o)), A::div(A::mul(p.ce[q], dhy_x), dx, rdx));
+          if (wpsi) {
+            p.psin[EY][AX][sd_][o] = vy;
+            p.psin[EZ][AX][sd_][o] = vz;
           }
-          const int q = sq(ze_code);
-          const long long o = psi_idx3(AZ, i, y, sd(ze_code), p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.be[q], p.psi[EX][AZ][ss(ze_code)][o]),
-                             A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
-          if (wpsi) p.psin[EX][AZ][ss(ze_code)][o] = v;
-          e = A::sub(e, A::mul(cb, v));
+          ney = A::sub(ney, A::mul(cb1, vy));
+          nez = A::add(nez, A::mul(cb2, vz));
         }
-        e0 = e;
-        me |= 1;
-      }
-      if (i_c && ey_jk) {  // Ey                                     :53-60, 104-110, 139-162
-        const T cb = cur[(6 + 1) * BOXS + bo];
-        const T dhx = A::sub(cur[HX * BOXS + bo + 1], hx0);
-        const T dhz = A::sub(nxt[HZ * BOXS + bo], hz0);
-        T e = A::add(e1, A::mul(cb, A::sub(A::div(dhx, kze, rkze), A::div(dhz, kxe, rkxe))));
-        if (p.src_field == EY && src_i && src_jk) e = A::sub(e, Jn);
-        if (xe_code >= 0) {
-          const int q = sq(xe_code);
-          const long long o = psi_idx3(AX, sd(xe_code), y, z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.be[q], p.psi[EY][AX][ss(xe_code)][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
-          if (wpsi) p.psin[EY][AX][ss(xe_code)][o] = v;
-          e = A::sub(e, A::mul(cb, v));
-        }
-        if (ze_code >= 0) {
-          const int q = sq(ze_code);
-          const long long o = psi_idx3(AZ, i, y, sd(ze_code), p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.be[q], p.psi[EY][AZ][ss(ze_code)][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
-          if (wpsi) p.psin[EY][AZ][ss(ze_code)][o] = v;
-          e = A::add(e, A::mul(cb, v));
-        }
-        e1 = e;
-        me |= 2;
-      }
-      if (i_c && ez_jk) {  // Ez                                     :63-70, 165-188
-        const T cb = cur[(6 + 2) * BOXS + bo];
-        const T hy1 = nxt[HY * BOXS + bo];
-        const T dhy = A::sub(hy1, hy0);
-        const T dhx = A::sub(cur[HX * BOXS + bo + BZ], hx0);
-        T e = A::add(e2, A::mul(cb, A::sub(A::div(dhy, kxe, rkxe), A::div(dhx, kye, rkye))));
-        if (xe_code >= 0) {
-          T h1 = hy1, h0 = hy0;
-          if (p.src_field == HY) {
-            if (src_i1 && src_jk) h1 = A::sub(h1, Jn);
-            if (src_i && src_jk) h0 = A::sub(h0, Jn);
+        e0 = i_o ? nex : e0;
+        e1 = i_c ? ney : e1;
+        e2 = i_c ? nez : e2;
+      } else {
+        if (ok && (slab_yz || xe_code >= 0)) {
+          // Hy differences seen by the CPML of Ex (along z) and Ez (along x): the
+          // Hy source is applied between the E curl and the E CPML
+          T dhy_zs = dhy_z, dhy_xs = dhy_x;
+          if (src_p && p.src_field == HY) {
+            const T jz1 = (src_i && src_jk1) ? Jn : T(0), jz0 = (src_i && src_jk) ? Jn : T(0);
+            const T jx1 = (src_i1 && src_jk) ? Jn : T(0);
+            dhy_zs = A::sub(A::sub(hy_z1, jz1), A::sub(hy0, jz0));
+            dhy_xs = A::sub(A::sub(hy_x1, jx1), A::sub(hy0, jz0));
           }
-          const int q = sq(xe_code);
-          const long long o = psi_idx3(AX, sd(xe_code), y, z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.be[q], p.psi[EZ][AX][ss(xe_code)][o]),
-                             A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
-          if (wpsi) p.psin[EZ][AX][ss(xe_code)][o] = v;
-          e = A::add(e, A::mul(cb, v));
+          // all old psi values first (read-only in this launch), then the updates
+          const long long b_ax = xe_code >= 0 ? (long long)sd(xe_code) * plane_ax : 0;
+          const bool a_xy = mex && ye_code >= 0, a_xz = mex && ze_code >= 0, a_yx = mey && xe_code >= 0;
+          const bool a_yz = mey && ze_code >= 0, a_zx = mez && xe_code >= 0, a_zy = mez && ye_code >= 0;
+          const T v_xy = a_xy ? __ldg(p.psi[EX][AY][ss(ye_code)] + (b_ay + o_ay_e)) : T(0);
+          const T v_xz = a_xz ? __ldg(p.psi[EX][AZ][ss(ze_code)] + (b_az + o_az_e)) : T(0);
+          const T v_yx = a_yx ? __ldg(p.psi[EY][AX][ss(xe_code)] + (b_ax + off_ax)) : T(0);
+          const T v_yz = a_yz ? __ldg(p.psi[EY][AZ][ss(ze_code)] + (b_az + o_az_e)) : T(0);
+          const T v_zx = a_zx ? __ldg(p.psi[EZ][AX][ss(xe_code)] + (b_ax + off_ax)) : T(0);
+          const T v_zy = a_zy ? __ldg(p.psi[EZ][AY][ss(ye_code)] + (b_ay + o_ay_e)) : T(0);
+          if (a_xy) {  // update_pml_ex_yinc
+            const int q = sq(ye_code);
+            const T v = A::add(A::mul(p.be[q], v_xy), A::div(A::mul(p.ce[q], dhz_y), dx, rdx));
+            if (wpsi) p.psin[EX][AY][ss(ye_code)][b_ay + o_ay_e] = v;
+            nex = A::add(nex, A::mul(cb0, v));
+          }
+          if (a_xz) {  // update_pml_ex_zinc
+            const int q = sq(ze_code);
+            const T v = A::add(A::mul(p.be[q], v_xz), A::div(A::mul(p.ce[q], dhy_zs), dx, rdx));
+            if (wpsi) p.psin[EX][AZ][ss(ze_code)][b_az + o_az_e] = v;
+            nex = A::sub(nex, A::mul(cb0, v));
+          }
+          if (a_yx) {  // update_pml_ey_xinc
+            const int q = sq(xe_code);
+            const T v = A::add(A::mul(p.be[q], v_yx), A::div(A::mul(p.ce[q], dhz_x), dx, rdx));
+            if (wpsi) p.psin[EY][AX][ss(xe_code)][b_ax + off_ax] = v;
+            ney = A::sub(ney, A::mul(cb1, v));
+          }
+          if (a_yz) {  // update_pml_ey_zinc
+            const int q = sq(ze_code);
+            const T v = A::add(A::mul(p.be[q], v_yz), A::div(A::mul(p.ce[q], dhx_z), dx, rdx));
+            if (wpsi) p.psin[EY][AZ][ss(ze_code)][b_az + o_az_e] = v;
+            ney = A::add(ney, A::mul(cb1, v));
+          }
+          if (a_zx) {  // update_pml_ez_xinc
+            const int q = sq(xe_code);
+            const T v = A::add(A::mul(p.be[q], v_zx), A::div(A::mul(p.ce[q], dhy_xs), dx, rdx));
+            if (wpsi) p.psin[EZ][AX][ss(xe_code)][b_ax + off_ax] = v;
+            nez = A::add(nez, A::mul(cb2, v));
+          }
+          if (a_zy) {  // update_pml_ez_yinc
+            const int q = sq(ye_code);
+            const T v = A::add(A::mul(p.be[q], v_zy), A::div(A::mul(p.ce[q], dhx_y), dx, rdx));
+            if (wpsi) p.psin[EZ][AY][ss(ye_code)][b_ay + o_ay_e] = v;
+            nez = A::sub(nez, A::mul(cb2, v));
+          }
         }
-        if (ye_code >= 0) {
-          const int q = sq(ye_code);
-          const long long o = psi_idx3(AY, i, sd(ye_code), z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.be[q], p.psi[EZ][AY][ss(ye_code)][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
-          if (wpsi) p.psin[EZ][AY][ss(ye_code)][o] = v;
-          e = A::sub(e, A::mul(cb, v));
+        if (edge_p) {
+          e0 = mex ? nex : e0;
+          e1 = mey ? ney : e1;
+          e2 = mez ? nez : e2;
+        } else {
+          e0 = nex;
+          e1 = ney;
+          e2 = nez;
         }
-        e2 = e;
-        me |= 4;
+      }
+      enew[tid] = e0;
+      enew[NT + tid] = e1;
+      enew[2 * NT + tid] = e2;
+      if (!ok) s_abort[u & 1] = 1;
+      __syncthreads();  // new E of the tile visible; stage sc no longer read
+      if (s_abort[u & 1]) {
+        aborted = true;
+        break;
+      }
+      if (tid == 0 && u + S < nplanes) {
+        issue(u + S);  // into stage sc
+        s_issued = u + S + 1;
+      }
+      // ---- new H of owned cells; store E and H ------------------------------------
+      // fdtd_funcs.py:73-100 (curl), :83-90 (Hy source before update_hy), :191-266 (CPML)
+      if (i >= x0) {
+        // halo cells (row 0 / column 0 of the E box) compute too and store nothing
+        const T dey_z = A::sub(e1, enew[NT + tid - 1]);
+        const T dez_y = A::sub(e2, enew[2 * NT + tid - TBZ]);
+        const T dez_x = A::sub(e2, ez_prev);
+        const T dex_z = A::sub(e0, enew[tid - 1]);
+        const T dex_y = A::sub(e0, enew[tid - TBZ]);
+        const T dey_x = A::sub(e1, ey_prev);
+        T hy_s = hy0;
+        if (src_i && p.src_field == HY && src_jk) hy_s = A::sub(hy_s, Jn);
+        T nhx = A::add(hx0, A::mul(db, A::sub(A::div(dey_z, kzh, rkzh), A::div(dez_y, kyh, rkyh))));
+        T nhy = A::add(hy_s, A::mul(db, A::sub(A::div(dez_x, kxh, rkxh), A::div(dex_z, kzh, rkzh))));
+        T nhz = A::add(hz0, A::mul(db, A::sub(A::div(dex_y, kyh, rkyh), A::div(dey_x, kxh, rkxh))));
+        const bool mhx = own && i_c && hx_jk, mhy = own && i_o && hy_jk, mhz = own && i_o && hz_jk;
+        T h0v, h1v, h2v;
+        if (CLEAN) {
+          if (xh_code >= 0 && i_o && own) {  // update_pml_hy_xinc, update_pml_hz_xinc (in place)
+            const int q = sq(xh_code), sd_ = ss(xh_code);
+            const long long o = (long long)sd(xh_code) * plane_ax + off_ax;
+            T *const py = p.psi[HY][AX][sd_] + o;
+            T *const pz = p.psi[HZ][AX][sd_] + o;
+            const T oy = *py, oz = *pz;
+            const T vy = A::add(A::mul(p.bh[q], oy), A::div(A::mul(p.ch[q], dez_x), dx, rdx));
+            const T vz = A::add(A::mul(p.bh[q], oz), A::div(A::mul(p.ch[q], dey_x), dx, rdx));
+            *py = vy;
+            *pz = vz;
+            nhy = A::add(nhy, A::mul(db, vy));
+            nhz = A::sub(nhz, A::mul(db, vz));
+          }
+          h0v = i_c ? nhx : hx0;
+          h1v = i_o ? nhy : hy0;
+          h2v = i_o ? nhz : hz0;
+        } else {
+          if (slab_yz || xh_code >= 0) {
+            // H psi is updated in place, each element by its own cell only: loads first
+            const long long b_ax = xh_code >= 0 ? (long long)sd(xh_code) * plane_ax : 0;
+            const bool a_xy = mhx && yh_code >= 0, a_xz = mhx && zh_code >= 0, a_yx = mhy && xh_code >= 0;
+            const bool a_yz = mhy && zh_code >= 0, a_zx = mhz && xh_code >= 0, a_zy = mhz && yh_code >= 0;
+            T *const q_xy = p.psi[HX][AY][a_xy ? ss(yh_code) : 0] + (b_ay + o_ay_h);
+            T *const q_xz = p.psi[HX][AZ][a_xz ? ss(zh_code) : 0] + (b_az + o_az_h);
+            T *const q_yx = p.psi[HY][AX][a_yx ? ss(xh_code) : 0] + (b_ax + off_ax);
+            T *const q_yz = p.psi[HY][AZ][a_yz ? ss(zh_code) : 0] + (b_az + o_az_h);
+            T *const q_zx = p.psi[HZ][AX][a_zx ? ss(xh_code) : 0] + (b_ax + off_ax);
+            T *const q_zy = p.psi[HZ][AY][a_zy ? ss(yh_code) : 0] + (b_ay + o_ay_h);
+            const T v_xy = a_xy ? *q_xy : T(0), v_xz = a_xz ? *q_xz : T(0), v_yx = a_yx ? *q_yx : T(0);
+            const T v_yz = a_yz ? *q_yz : T(0), v_zx = a_zx ? *q_zx : T(0), v_zy = a_zy ? *q_zy : T(0);
+            if (a_xy) {  // update_pml_hx_yinc
+              const int q = sq(yh_code);
+              const T v = A::add(A::mul(p.bh[q], v_xy), A::div(A::mul(p.ch[q], dez_y), dx, rdx));
+              *q_xy = v;
+              nhx = A::sub(nhx, A::mul(db, v));
+            }
+            if (a_xz) {  // update_pml_hx_zinc
+              const int q = sq(zh_code);
+              const T v = A::add(A::mul(p.bh[q], v_xz), A::div(A::mul(p.ch[q], dey_z), dx, rdx));
+              *q_xz = v;
+              nhx = A::add(nhx, A::mul(db, v));
+            }
+            if (a_yx) {  // update_pml_hy_xinc
+              const int q = sq(xh_code);
+              const T v = A::add(A::mul(p.bh[q], v_yx), A::div(A::mul(p.ch[q], dez_x), dx, rdx));
+              *q_yx = v;
+              nhy = A::add(nhy, A::mul(db, v));
+            }
+            if (a_yz) {  // update_pml_hy_zinc
+              const int q = sq(zh_code);
+              const T v = A::add(A::mul(p.bh[q], v_yz), A::div(A::mul(p.ch[q], dex_z), dx, rdx));
+              *q_yz = v;
+              nhy = A::sub(nhy, A::mul(db, v));
+            }
+            if (a_zx) {  // update_pml_hz_xinc
+              const int q = sq(xh_code);
+              const T v = A::add(A::mul(p.bh[q], v_zx), A::div(A::mul(p.ch[q], dey_x), dx, rdx));
+              *q_zx = v;
+              nhz = A::sub(nhz, A::mul(db, v));
+            }
+            if (a_zy) {  // update_pml_hz_yinc
+              const int q = sq(yh_code);
+              const T v = A::add(A::mul(p.bh[q], v_zy), A::div(A::mul(p.ch[q], dex_y), dx, rdx));
+              *q_zy = v;
+              nhz = A::add(nhz, A::mul(db, v));
+            }
+          }
+          if (edge_p) {
+            h0v = mhx ? nhx : hx0;
+            h1v = mhy ? nhy : hy0;
+            h2v = mhz ? nhz : hz0;
+          } else {
+            h0v = nhx;
+            h1v = nhy;
+            h2v = nhz;
+          }
+          if (capt) {
+            const T ev[3] = {e0, e1, e2}, hv[3] = {h0v, h1v, h2v};
+            const int me = (mex ? 1 : 0) | (mey ? 2 : 0) | (mez ? 4 : 0);
+            const int mh = (mhx ? 1 : 0) | (mhy ? 2 : 0) | (mhz ? 4 : 0);
+            y3_capture_e(p, s, i, y, z, me, ev);
+            y3_capture_h(p, s, i, y, z, mh, hv);
+          }
+        }
+        if (own) {
+          const long long g = (long long)i * plane_f + g_jk;
+          fEX[g] = e0;
+          fEY[g] = e1;
+          fEZ[g] = e2;
+          fHX[g] = h0v;
+          fHY[g] = h1v;
+          fHZ[g] = h2v;
+        }
+      }
+      ey_prev = e1;
+      ez_prev = e2;
+      sc = sn;
+      if (++sn == S) {
+        sn = 0;
+        pn ^= 1u;
       }
     }
-    enew[tid] = e0;
-    enew[NT + tid] = e1;
-    enew[2 * NT + tid] = e2;
-    if (!ok) s_abort = 1;
-    __syncthreads();  // new E of the tile visible; stage (u-1) % S no longer read
-    if (s_abort) break;
-    if (tid == 0 && u + S - 1 < nplanes) {
-      issue(u + S - 1);  // into stage (u-1) % S
-      s_issued = u + S;
-    }
-    // ---- new H of owned cells; store E and H ------------------------------------
-    if (own && i >= x0) {
-      T h0v = hx0, h1v = hy0, h2v = hz0;
-      int mh = 0;
-      const T db = p.db;
-      if (i_c && hx_jk) {  // Hx                                     :73-80, 191-214
-        const T dey = A::sub(e1, enew[NT + tid - 1]);
-        const T dez = A::sub(e2, enew[2 * NT + tid - TBZ]);
-        T h = A::add(h0v, A::mul(db, A::sub(A::div(dey, kzh, rkzh), A::div(dez, kyh, rkyh))));
-        if (yh_code >= 0) {
-          const int q = sq(yh_code);
-          T *ps = p.psi[HX][AY][ss(yh_code)] + psi_idx3(AY, i, sd(yh_code), z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
-          *ps = v;
-          h = A::sub(h, A::mul(db, v));
-        }
-        if (zh_code >= 0) {
-          const int q = sq(zh_code);
-          T *ps = p.psi[HX][AZ][ss(zh_code)] + psi_idx3(AZ, i, y, sd(zh_code), p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
-          *ps = v;
-          h = A::add(h, A::mul(db, v));
-        }
-        h0v = h;
-        mh |= 1;
-      }
-      if (i_o && hy_jk) {  // Hy                                     :83-90, 217-240
-        const T dez = A::sub(e2, ez_prev);
-        const T dex = A::sub(e0, enew[tid - 1]);
-        T h = h1v;
-        if (p.src_field == HY && src_i && src_jk) h = A::sub(h, Jn);  // source precedes update_hy
-        h = A::add(h, A::mul(db, A::sub(A::div(dez, kxh, rkxh), A::div(dex, kzh, rkzh))));
-        if (xh_code >= 0) {
-          const int q = sq(xh_code);
-          T *ps = p.psi[HY][AX][ss(xh_code)] + psi_idx3(AX, sd(xh_code), y, z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
-          *ps = v;
-          h = A::add(h, A::mul(db, v));
-        }
-        if (zh_code >= 0) {
-          const int q = sq(zh_code);
-          T *ps = p.psi[HY][AZ][ss(zh_code)] + psi_idx3(AZ, i, y, sd(zh_code), p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
-          *ps = v;
-          h = A::sub(h, A::mul(db, v));
-        }
-        h1v = h;
-        mh |= 2;
-      }
-      if (i_o && hz_jk) {  // Hz                                     :93-100, 243-266
-        const T dex = A::sub(e0, enew[tid - TBZ]);
-        const T dey = A::sub(e1, ey_prev);
-        T h = A::add(h2v, A::mul(db, A::sub(A::div(dex, kyh, rkyh), A::div(dey, kxh, rkxh))));
-        if (xh_code >= 0) {
-          const int q = sq(xh_code);
-          T *ps = p.psi[HZ][AX][ss(xh_code)] + psi_idx3(AX, sd(xh_code), y, z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
-          *ps = v;
-          h = A::sub(h, A::mul(db, v));
-        }
-        if (yh_code >= 0) {
-          const int q = sq(yh_code);
-          T *ps = p.psi[HZ][AY][ss(yh_code)] + psi_idx3(AY, i, sd(yh_code), z, p.nx, p.ny, p.nz, P);
-          const T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
-          *ps = v;
-          h = A::add(h, A::mul(db, v));
-        }
-        h2v = h;
-        mh |= 4;
-      }
-      const long long g = (long long)i * p.ny * p.nzp + g_jk;
-      p.fn[EX][g] = e0;
-      p.fn[EY][g] = e1;
-      p.fn[EZ][g] = e2;
-      p.fn[HX][g] = h0v;
-      p.fn[HY][g] = h1v;
-      p.fn[HZ][g] = h2v;
-      if (capt) {
-        const T ev[3] = {e0, e1, e2}, hv[3] = {h0v, h1v, h2v};
-        y3_capture_e(p, s, i, y, z, me, ev);
-        y3_capture_h(p, s, i, y, z, mh, hv);
-      }
-    }
-    ey_prev = e1;
-    ez_prev = e2;
-  }
-  if (s_abort && tid == 0) {
+  };
+  if (fl == 0)
+    march(std::true_type{});
+  else
+    march(std::false_type{});
+
+  if (aborted && tid == 0) {
     atomicExch(p.state + 1, 1);  // reported to the host by oidt_job_sync
     // copies issued after the failed one: bounded wait so none lands after exit
-    for (int u = s_failed; u < s_issued; ++u) (void)wait(u);
+    for (int v = s_failed; v < s_issued; ++v) (void)wait(v % S, (unsigned)((v / S) & 1));
   }
 }
 
