@@ -77,6 +77,10 @@ def _random_cases():
                                       core_x_nm=120, core_y_nm=160, sigma_nm=25, lc_nm=60, seed=5),
         "yee3d_tm": lambda: W.strip3d(nx=21, ny=24, nz=33, P=3, src_gap=2, port_gap=3, steps=40, nf=3,
                                       core_x_nm=140, core_y_nm=180, source="TM", seed=6),
+        # large enough that both 3D launch forms have interior work units with
+        # no CPML, edge or source cells (and a port plane inside one of them)
+        "yee3d_wide": lambda: W.strip3d(nx=30, ny=44, nz=130, P=4, src_gap=2, port_gap=26, steps=40, nf=3,
+                                        core_x_nm=160, core_y_nm=240, sigma_nm=20, lc_nm=60, seed=7),
     }
 
 
@@ -96,7 +100,8 @@ def _te2_spec():
     return s
 
 
-@pytest.mark.parametrize("name", ["tm2", "te2", "yee3d_te", "yee3d_tm", "yee3d_te_cell", "yee3d_tm_cell"])
+@pytest.mark.parametrize("name", ["tm2", "te2", "yee3d_te", "yee3d_tm", "yee3d_wide", "yee3d_te_cell",
+                                  "yee3d_tm_cell", "yee3d_wide_cell"])
 @pytest.mark.parametrize("ring", [1, 7, 32])
 def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     variant = "cell" if name.endswith("_cell") else "sweep"
