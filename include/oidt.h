@@ -98,8 +98,8 @@ typedef struct oidt_job_desc {
   /* float64 twiddles [nf][nt]: cos/sin(2 pi f n dt) and at (n + 1/2) dt */
   const double *cos_e, *sin_e, *cos_h, *sin_h;
   int32_t ring_steps; /* steps buffered between DFT folds (0 = default)    */
-  /* reserved[0]: 3D launch form, 0 = plane sweep (one launch per step),
-   *              1 = per-cell E-half / H-half launches;
+  /* reserved[0]: 3D launch form, 0 = per-cell E-half / H-half launches,
+   *              1 = plane sweep (one launch per step);
    * reserved[1]: 1 = launch every step directly (no CUDA-graph replay);
    * others must be 0. */
   int32_t reserved[7];

@@ -46,18 +46,18 @@ constexpr int kBlock3Z = 32, kBlock3Y = 4;
 constexpr int kBlock2 = 128;
 constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
 constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread box
-constexpr int kVariantSweep = 0, kVariantCell = 1;
+constexpr int kVariantCell = 0, kVariantSweep = 1;  // oidt_job_desc.reserved[0]
 
 // ---------------------------------------------------------------------------
 // Per-cell launches (2D, and the 3D per-cell variant): in place.
 // ---------------------------------------------------------------------------
 // A block of the 3D per-cell launches covers kBlock3Z (k) x kBlock3Y (j) cells
-// of one x-plane; each warp is one (i, j) row of 32 consecutive k.  Warps
-// whose cells all lie strictly inside the update ranges, outside the z CPML
-// slabs of the half-step and away from the source box run the lean body: the
-// three curl updates, then the x- and y-slab CPML terms, whose presence is the
-// same for the whole warp (operation order as y3_e_compute / y3_h_compute,
-// which they equal on such cells).  Other warps run the general per-cell code.
+// of one x-plane; each warp is one (i, j) row of 32 consecutive k.  Blocks
+// away from the source box run the range-masked body: the three curl
+// updates, then the CPML terms -- x and y slabs uniform over the warp, z slab
+// per lane -- with each component stored where its (i, j, k) range holds
+// (operation order as y3_e_compute / y3_h_compute, which they equal cell by
+// cell).  Blocks meeting the source box run the general per-cell code.
 template <typename T>
 __device__ __forceinline__ bool block_meets_src(const Params<T> &p, int i, int j0, int k0) {
   // the source box widened by one cell below in i and k (the E CPML of Ex and
@@ -66,106 +66,175 @@ __device__ __forceinline__ bool block_meets_src(const Params<T> &p, int i, int j
          k0 < p.shi[2] && k0 + kBlock3Z > p.slo[2] - 1;
 }
 
+// Interior warps address every grid array as (per-plane base, uniform over
+// the block) + (32-bit offset inside the plane), and the CPML slabs likewise;
+// plan_job rejects grids whose plane or slab sizes would not fit.
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(128) k_y3_e(Params<T> p, int s) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_e(Params<T> p, int s) {
   const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = blockIdx.z;
   const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
-  // E z slabs: [kb, kb+P) and [ke-P, ke)
-  const bool lean = i > p.ib && i < p.ie && j > p.jb && j < p.je && k0 >= p.kb + P && k0 + kBlock3Z <= p.ke - P &&
-                    !block_meets_src(p, i, j0, k0);
-  if (lean) {
+  if (!block_meets_src(p, i, j0, k0)) {
+    // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
+    // read below stays inside the grid arrays
+    if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
     using A = Ar<T, EXACT>;
-    const long long sy = p.nzp, sx = (long long)p.ny * p.nzp, c = i * sx + j * sy + k;
-    const T *hx = p.f[HX] + c, *hy = p.f[HY] + c, *hz = p.f[HZ] + c;
-    const T hx0 = __ldg(hx), hy0 = __ldg(hy), hz0 = __ldg(hz);
-    const T dhz_y = A::sub(__ldg(hz + sy), hz0), dhy_z = A::sub(__ldg(hy + 1), hy0);
-    const T dhx_z = A::sub(__ldg(hx + 1), hx0), dhz_x = A::sub(__ldg(hz + sx), hz0);
-    const T dhy_x = A::sub(__ldg(hy + sx), hy0), dhx_y = A::sub(__ldg(hx + sy), hx0);
+    const int sy = p.nzp, nz = p.nz;
+    const long long sx = (long long)p.ny * p.nzp, bi = i * sx;
+    const int o = j * sy + k;  // offset inside the plane
+    const T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
+    const T hx0 = __ldg(hx + o), hy0 = __ldg(hy + o), hz0 = __ldg(hz + o);
+    const T dhz_y = A::sub(__ldg(hz + (o + sy)), hz0), dhy_z = A::sub(__ldg(hy + (o + 1)), hy0);
+    const T dhx_z = A::sub(__ldg(hx + (o + 1)), hx0), dhz_x = A::sub(__ldg(hz + sx + o), hz0);
+    const T dhy_x = A::sub(__ldg(hy + sx + o), hy0), dhx_y = A::sub(__ldg(hx + (o + sy)), hx0);
     const T rkx = p.rkd[0][i], rky = p.rkd[1][j], rkz = p.rkd[2][k];
     const T kx = EXACT ? p.kd[0][i] : T(0), ky = EXACT ? p.kd[1][j] : T(0), kz = EXACT ? p.kd[2][k] : T(0);
-    const T cb0 = __ldg(p.cb[0] + c), cb1 = __ldg(p.cb[1] + c), cb2 = __ldg(p.cb[2] + c);
+    const T cb0 = __ldg(p.cb[0] + bi + o), cb1 = __ldg(p.cb[1] + bi + o), cb2 = __ldg(p.cb[2] + bi + o);
+    T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
     T e[3];
-    e[0] = A::add(p.f[EX][c], A::mul(cb0, A::sub(A::div(dhz_y, ky, rky), A::div(dhy_z, kz, rkz))));
-    e[1] = A::add(p.f[EY][c], A::mul(cb1, A::sub(A::div(dhx_z, kz, rkz), A::div(dhz_x, kx, rkx))));
-    e[2] = A::add(p.f[EZ][c], A::mul(cb2, A::sub(A::div(dhy_x, kx, rkx), A::div(dhx_y, ky, rky))));
+    e[0] = A::add(ex[o], A::mul(cb0, A::sub(A::div(dhz_y, ky, rky), A::div(dhy_z, kz, rkz))));
+    e[1] = A::add(ey[o], A::mul(cb1, A::sub(A::div(dhx_z, kz, rkz), A::div(dhz_x, kx, rkx))));
+    e[2] = A::add(ez[o], A::mul(cb2, A::sub(A::div(dhy_x, kx, rkx), A::div(dhx_y, ky, rky))));
+    // updated components: Ex i (ib,ie) j [jb,je) k [kb,ke); Ey i [ib,ie) j (jb,je) k [kb,ke);
+    // Ez i [ib,ie) j [jb,je) k (kb,ke)
+    const bool kc = k >= p.kb && k < p.ke, ko = k > p.kb && k < p.ke;
+    const bool mex = i > p.ib && kc, mey = j > p.jb && kc, mez = ko;
     int d, side, q;
     if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc, update_pml_ez_xinc
-      const long long o = psi_idx3(AX, d, j, k, p.nx, p.ny, p.nz, P);
-      T *const py = p.psi[EY][AX][side] + o, *const pz = p.psi[EZ][AX][side] + o;
-      const T vy = A::add(A::mul(p.be[q], *py), A::div(A::mul(p.ce[q], dhz_x), p.dx, p.rdx));
-      const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhy_x), p.dx, p.rdx));
-      *py = vy;
-      *pz = vz;
-      e[1] = A::sub(e[1], A::mul(cb1, vy));
-      e[2] = A::add(e[2], A::mul(cb2, vz));
+      const int oa = (d * p.ny + j) * nz + k;
+      if (mey) {
+        T *const py = p.psi[EY][AX][side] + oa;
+        const T vy = A::add(A::mul(p.be[q], *py), A::div(A::mul(p.ce[q], dhz_x), p.dx, p.rdx));
+        *py = vy;
+        e[1] = A::sub(e[1], A::mul(cb1, vy));
+      }
+      if (mez) {
+        T *const pz = p.psi[EZ][AX][side] + oa;
+        const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhy_x), p.dx, p.rdx));
+        *pz = vz;
+        e[2] = A::add(e[2], A::mul(cb2, vz));
+      }
     }
     if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc, update_pml_ez_yinc
-      const long long o = psi_idx3(AY, i, d, k, p.nx, p.ny, p.nz, P);
-      T *const px = p.psi[EX][AY][side] + o, *const pz = p.psi[EZ][AY][side] + o;
-      const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhz_y), p.dx, p.rdx));
-      const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhx_y), p.dx, p.rdx));
-      *px = vx;
-      *pz = vz;
-      e[0] = A::add(e[0], A::mul(cb0, vx));
-      e[2] = A::sub(e[2], A::mul(cb2, vz));
+      const int oa = (i * P + d) * nz + k;
+      if (mex) {
+        T *const px = p.psi[EX][AY][side] + oa;
+        const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhz_y), p.dx, p.rdx));
+        *px = vx;
+        e[0] = A::add(e[0], A::mul(cb0, vx));
+      }
+      if (mez) {
+        T *const pz = p.psi[EZ][AY][side] + oa;
+        const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhx_y), p.dx, p.rdx));
+        *pz = vz;
+        e[2] = A::sub(e[2], A::mul(cb2, vz));
+      }
     }
-    p.f[EX][c] = e[0];
-    p.f[EY][c] = e[1];
-    p.f[EZ][c] = e[2];
-    if (k == p.port_pos[0] || k == p.port_pos[1]) y3_capture_e(p, s, i, j, k, 7, e);
+    if (kc && (q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ex_zinc, update_pml_ey_zinc
+      const int oa = (i * p.ny + j) * P + d;
+      if (mex) {
+        T *const px = p.psi[EX][AZ][side] + oa;
+        const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhy_z), p.dx, p.rdx));
+        *px = vx;
+        e[0] = A::sub(e[0], A::mul(cb0, vx));
+      }
+      if (mey) {
+        T *const py = p.psi[EY][AZ][side] + oa;
+        const T vy = A::add(A::mul(p.be[q], *py), A::div(A::mul(p.ce[q], dhx_z), p.dx, p.rdx));
+        *py = vy;
+        e[1] = A::add(e[1], A::mul(cb1, vy));
+      }
+    }
+    if (mex) ex[o] = e[0];
+    if (mey) ey[o] = e[1];
+    if (mez) ez[o] = e[2];
+    if (k == p.port_pos[0] || k == p.port_pos[1])
+      y3_capture_e(p, s, i, j, k, (mex ? 1 : 0) | (mey ? 2 : 0) | (mez ? 4 : 0), e);
     return;
   }
   if (k >= p.nz || j >= p.ny) return;
   y3_e_cell<T, EXACT>(p, i, j, k, p.state[0] + s, s);
 }
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(128) k_y3_h(Params<T> p, int s) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_h(Params<T> p, int s) {
   const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = blockIdx.z;
   const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
-  // H z slabs: (kb, kb+P) and (ke-P, ke)
-  const bool lean = i > p.ib && i < p.ie && j > p.jb && j < p.je && k0 >= p.kb + P &&
-                    k0 + kBlock3Z - 1 <= p.ke - P && !block_meets_src(p, i, j0, k0);
-  if (lean) {
+  if (!block_meets_src(p, i, j0, k0)) {
+    // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
+    // read below stays inside the grid arrays (ib, jb >= 1)
+    if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
     using A = Ar<T, EXACT>;
-    const long long sy = p.nzp, sx = (long long)p.ny * p.nzp, c = i * sx + j * sy + k;
-    const T *ex = p.f[EX] + c, *ey = p.f[EY] + c, *ez = p.f[EZ] + c;
-    const T ex0 = __ldg(ex), ey0 = __ldg(ey), ez0 = __ldg(ez);
-    const T dey_z = A::sub(ey0, __ldg(ey - 1)), dez_y = A::sub(ez0, __ldg(ez - sy));
-    const T dez_x = A::sub(ez0, __ldg(ez - sx)), dex_z = A::sub(ex0, __ldg(ex - 1));
-    const T dex_y = A::sub(ex0, __ldg(ex - sy)), dey_x = A::sub(ey0, __ldg(ey - sx));
+    const int sy = p.nzp, nz = p.nz;
+    const long long sx = (long long)p.ny * p.nzp, bi = i * sx;
+    const int o = j * sy + k;  // offset inside the plane
+    const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
+    // updated components: Hx i [ib,ie) j (jb,je) k (kb,ke); Hy i (ib,ie) j [jb,je) k (kb,ke);
+    // Hz i (ib,ie) j (jb,je) k [kb,ke)
+    const bool ko = k > p.kb && k < p.ke, kc = k >= p.kb && k < p.ke;
+    const bool mhx = j > p.jb && ko, mhy = i > p.ib && ko, mhz = i > p.ib && j > p.jb && kc;
+    const T ex0 = __ldg(ex + o), ey0 = __ldg(ey + o), ez0 = __ldg(ez + o);
+    // (k - 1 is read only where k > kb >= 1)
+    const T dey_z = A::sub(ey0, ko ? __ldg(ey + (o - 1)) : ey0), dez_y = A::sub(ez0, __ldg(ez + (o - sy)));
+    const T dez_x = A::sub(ez0, __ldg(ez - sx + o)), dex_z = A::sub(ex0, ko ? __ldg(ex + (o - 1)) : ex0);
+    const T dex_y = A::sub(ex0, __ldg(ex + (o - sy))), dey_x = A::sub(ey0, __ldg(ey - sx + o));
     const T rkx = p.rkd[3][i], rky = p.rkd[4][j], rkz = p.rkd[5][k];
     const T kx = EXACT ? p.kd[3][i] : T(0), ky = EXACT ? p.kd[4][j] : T(0), kz = EXACT ? p.kd[5][k] : T(0);
     const T db = p.db;
+    T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
     T h[3];
-    h[0] = A::add(p.f[HX][c], A::mul(db, A::sub(A::div(dey_z, kz, rkz), A::div(dez_y, ky, rky))));
-    h[1] = A::add(p.f[HY][c], A::mul(db, A::sub(A::div(dez_x, kx, rkx), A::div(dex_z, kz, rkz))));
-    h[2] = A::add(p.f[HZ][c], A::mul(db, A::sub(A::div(dex_y, ky, rky), A::div(dey_x, kx, rkx))));
+    h[0] = A::add(hx[o], A::mul(db, A::sub(A::div(dey_z, kz, rkz), A::div(dez_y, ky, rky))));
+    h[1] = A::add(hy[o], A::mul(db, A::sub(A::div(dez_x, kx, rkx), A::div(dex_z, kz, rkz))));
+    h[2] = A::add(hz[o], A::mul(db, A::sub(A::div(dex_y, ky, rky), A::div(dey_x, kx, rkx))));
     int d, side, q;
     if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hy_xinc, update_pml_hz_xinc
-      const long long o = psi_idx3(AX, d, j, k, p.nx, p.ny, p.nz, P);
-      T *const py = p.psi[HY][AX][side] + o, *const pz = p.psi[HZ][AX][side] + o;
-      const T vy = A::add(A::mul(p.bh[q], *py), A::div(A::mul(p.ch[q], dez_x), p.dx, p.rdx));
-      const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dey_x), p.dx, p.rdx));
-      *py = vy;
-      *pz = vz;
-      h[1] = A::add(h[1], A::mul(db, vy));
-      h[2] = A::sub(h[2], A::mul(db, vz));
+      const int oa = (d * p.ny + j) * nz + k;
+      if (mhy) {
+        T *const py = p.psi[HY][AX][side] + oa;
+        const T vy = A::add(A::mul(p.bh[q], *py), A::div(A::mul(p.ch[q], dez_x), p.dx, p.rdx));
+        *py = vy;
+        h[1] = A::add(h[1], A::mul(db, vy));
+      }
+      if (mhz) {
+        T *const pz = p.psi[HZ][AX][side] + oa;
+        const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dey_x), p.dx, p.rdx));
+        *pz = vz;
+        h[2] = A::sub(h[2], A::mul(db, vz));
+      }
     }
     if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc, update_pml_hz_yinc
-      const long long o = psi_idx3(AY, i, d, k, p.nx, p.ny, p.nz, P);
-      T *const px = p.psi[HX][AY][side] + o, *const pz = p.psi[HZ][AY][side] + o;
-      const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dez_y), p.dx, p.rdx));
-      const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dex_y), p.dx, p.rdx));
-      *px = vx;
-      *pz = vz;
-      h[0] = A::sub(h[0], A::mul(db, vx));
-      h[2] = A::add(h[2], A::mul(db, vz));
+      const int oa = (i * P + d) * nz + k;
+      if (mhx) {
+        T *const px = p.psi[HX][AY][side] + oa;
+        const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dez_y), p.dx, p.rdx));
+        *px = vx;
+        h[0] = A::sub(h[0], A::mul(db, vx));
+      }
+      if (mhz) {
+        T *const pz = p.psi[HZ][AY][side] + oa;
+        const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dex_y), p.dx, p.rdx));
+        *pz = vz;
+        h[2] = A::add(h[2], A::mul(db, vz));
+      }
     }
-    p.f[HX][c] = h[0];
-    p.f[HY][c] = h[1];
-    p.f[HZ][c] = h[2];
+    if (ko && (q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hx_zinc, update_pml_hy_zinc
+      const int oa = (i * p.ny + j) * P + d;
+      if (mhx) {
+        T *const px = p.psi[HX][AZ][side] + oa;
+        const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dey_z), p.dx, p.rdx));
+        *px = vx;
+        h[0] = A::add(h[0], A::mul(db, vx));
+      }
+      if (mhy) {
+        T *const py = p.psi[HY][AZ][side] + oa;
+        const T vy = A::add(A::mul(p.bh[q], *py), A::div(A::mul(p.ch[q], dex_z), p.dx, p.rdx));
+        *py = vy;
+        h[1] = A::sub(h[1], A::mul(db, vy));
+      }
+    }
+    if (mhx) hx[o] = h[0];
+    if (mhy) hy[o] = h[1];
+    if (mhz) hz[o] = h[2];
     if (k == p.port_pos[0] || k == p.port_pos[1] || k == p.port_pos[0] + 1 || k == p.port_pos[1] + 1)
-      y3_capture_h(p, s, i, j, k, 7, h);
+      y3_capture_h(p, s, i, j, k, (mhx ? 1 : 0) | (mhy ? 2 : 0) | (mhz ? 4 : 0), h);
     return;
   }
   if (k >= p.nz || j >= p.ny) return;
@@ -467,7 +536,13 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
         return bad("source box must lie inside the updated interior");
     }
   }
-  const int variant = is3 ? (d->reserved[0] == kVariantCell ? kVariantCell : kVariantSweep) : kVariantCell;
+  if (is3) {  // the 3D kernels address a plane and each CPML slab layer set with 32-bit offsets
+    const long long lim = 0x7fffffffLL, nzp4 = align_up(d->nz, 4);
+    if ((long long)d->ny * nzp4 > lim || (long long)P * d->ny * d->nz > lim || (long long)d->nx * P * d->nz > lim ||
+        (long long)d->nx * d->ny * P > lim)
+      return bad("grid too large: an x-plane or a CPML slab holds 2^31 or more elements");
+  }
+  const int variant = is3 && d->reserved[0] == kVariantSweep ? kVariantSweep : kVariantCell;
   const int esz = d->precision == OIDT_F32 ? 4 : 8;
   const int nzp = is3 ? (int)align_up(d->nz, 4) : 1;
   const long long N = (long long)d->nx * d->ny * nzp;

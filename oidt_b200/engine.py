@@ -130,7 +130,7 @@ class Engine:
         return b.value
 
     def submit(self, spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0,
-               variant: str = "sweep", graphs: bool = True) -> "Job":
+               variant: str = "cell", graphs: bool = True) -> "Job":
         d, keep = to_desc(spec, arith=arith, precision=precision, ring_steps=ring_steps, variant=variant,
                           graphs=graphs)
         jid = C.c_uint64()

@@ -1,7 +1,7 @@
 """Small fixed workloads for profiler captures (ncu launch lists and
 single-kernel captures).
 
-    python -m oidt_b200.prof --workload strip3d --steps 64 [--variant sweep|cell] [--no-graphs]
+    python -m oidt_b200.prof --workload strip3d --steps 64 [--variant cell|sweep] [--no-graphs]
 
 Runs the named workload for a few hundred launches and exits; the device
 state of the default 3D case (128 x 128 x 256 cells, FP32) is about 0.4 GB,
@@ -21,7 +21,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="strip3d", choices=("strip3d", "slab2d", "strip3d_large"))
     ap.add_argument("--steps", type=int, default=64)
-    ap.add_argument("--variant", default="sweep", choices=("sweep", "cell"))
+    ap.add_argument("--variant", default="cell", choices=("cell", "sweep"))
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--precision", default="float32", choices=("float32", "float64"))
     a = ap.parse_args(argv)

@@ -84,17 +84,17 @@ class JobDesc(C.Structure):
     ]
 
 
-VARIANTS = {"sweep": 0, "cell": 1}
+VARIANTS = {"cell": 0, "sweep": 1}
 
 
-def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "sweep",
+def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "cell",
             graphs: bool = True):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
     ``keepalive`` must outlive the ``oidt_job_create`` call.
 
-    ``variant`` (3D only): 'sweep' -- one plane-sweep launch per step (E and
-    H fused, TMA-staged tiles); 'cell' -- the per-cell E-half / H-half
-    launches.  2D jobs always use the per-cell launches.  ``graphs=False``
+    ``variant`` (3D only): 'cell' (default) -- the per-cell E-half / H-half
+    launches; 'sweep' -- one plane-sweep launch per step (E and H fused,
+    TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
     launches every step directly instead of replaying K-step CUDA graphs."""
     prec = np.dtype(precision if precision is not None else spec.precision)
     if prec not in (np.dtype(np.float32), np.dtype(np.float64)):

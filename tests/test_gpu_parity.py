@@ -179,9 +179,10 @@ def test_fp32_slab2d_full_run_within_targets(eng):
     job.release()
 
 
-def test_fp32_strip3d_within_targets(eng):
+@pytest.mark.parametrize("variant", ["cell", "sweep"])
+def test_fp32_strip3d_within_targets(eng, variant):
     """A reduced 3D rough strip (64 x 56 x 120, 700 steps) in float32 vs the
-    float64 oracle on identical inputs."""
+    float64 oracle on identical inputs, both 3D launch forms."""
     from oidt_b200 import workloads as W
     from oidt_b200.sparams import forward_s
     from tests.helpers import dft_dict_oracle
@@ -191,7 +192,7 @@ def test_fp32_strip3d_within_targets(eng):
     out = {}
     from oracle import cpu as OC
     for tag, spec in (("i", spec_i), ("r", spec_r)):
-        job = eng.submit(spec, arith="fast", precision=np.float32)
+        job = eng.submit(spec, arith="fast", precision=np.float32, variant=variant)
         job.run().sync(120000)
         s = oracle_from_spec(spec)
         OC.run_c(s, spec.nt)
