@@ -150,6 +150,20 @@ int32_t oidt_job_query(oidt_ctx *ctx, uint64_t job, int32_t *steps_done, int32_t
 int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t comp,
                           double *out_re_im, size_t n_doubles);
 
+/* Port-window DFT of one (port, comp), as oidt_job_read_dft but restricted
+ * to the DFT window [win_lo, win_hi): out = complex128 [nf][wi][wj] (3D, wi =
+ * win_hi[0] - win_lo[0], wj = win_hi[1] - win_lo[1]) or [nf][wj] (2D),
+ * interleaved re/im, n = number of doubles.  Allocates nothing: it stages
+ * through a fixed 16 MiB static device buffer (larger windows are rejected
+ * with OIDT_ERR_INVALID), for callers whose call path may not allocate
+ * device memory.  The first call on a device resolves the buffer's address
+ * (cudaGetSymbolAddress, which may load the module) and should come before
+ * any stream capture on that device.  The buffer is shared by all contexts
+ * on a device: calls on one device must not overlap.  No counterpart in the
+ * reference (its DFT arrays come back whole, fdtd_main.py:349-386). */
+int32_t oidt_job_read_dft_window_static(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t comp,
+                                        double *out, size_t n);
+
 /* Field snapshot / overwrite (reference layout, job precision). */
 int32_t oidt_job_read_field(oidt_ctx *ctx, uint64_t job, int32_t field, void *out, size_t nbytes);
 int32_t oidt_job_write_field(oidt_ctx *ctx, uint64_t job, int32_t field, const void *src, size_t nbytes);

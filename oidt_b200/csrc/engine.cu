@@ -1326,6 +1326,74 @@ int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t com
   return OIDT_OK;
 }
 
+// ---- port-window DFT readout through static device scratch -------------------
+// A variant of the staged readout that allocates nothing: the window of one
+// (port, component) accumulator is gathered into a file-scope device buffer of
+// fixed size and copied to the host from there.  Every element of the
+// gathered range is written before it is read, so nothing in the buffer has
+// to start at zero.  The buffer is shared by every context on a device, so
+// calls on one device must not overlap (calls through one context are
+// serialised by its mutex).
+namespace {
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB: 1 Mi complex doubles
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+std::mutex g_static_mu;
+constexpr int kMaxDevices = 64;
+void *g_static_addr[kMaxDevices] = {};  // resolved once per device
+
+__global__ void k_gather_window(const double2 *__restrict__ acc, double2 *__restrict__ dst, int nf, long long plane,
+                                int ny, int i0, int wi, int j0, int wj) {
+  const long long n = (long long)nf * wi * wj;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int jj = (int)(t % wj);
+    const long long r = t / wj;
+    const int ii = (int)(r % wi), f = (int)(r / wi);
+    dst[t] = acc[f * plane + (long long)(i0 + ii) * ny + (j0 + jj)];
+  }
+}
+}  // namespace
+
+int32_t oidt_job_read_dft_window_static(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t comp, double *out,
+                                        size_t n) {
+  if (!ctx || !out) return OIDT_ERR_INVALID;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  Job *J = find(ctx, job);
+  if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
+  const int nc = ncomp_of(J->d.mode);
+  if (port < 0 || port > 1 || comp < 0 || comp >= nc) return fail(ctx, OIDT_ERR_INVALID, "bad port/comp");
+  const bool is3 = J->d.mode == OIDT_MODE_YEE3D;
+  const int i0 = is3 ? J->d.win_lo[0] : 0, wi = is3 ? J->d.win_hi[0] - J->d.win_lo[0] : 1;
+  const int j0 = J->d.win_lo[1], wj = J->d.win_hi[1] - J->d.win_lo[1];
+  const size_t cells = (size_t)J->d.nf * wi * wj, need = 2 * cells;
+  if (n < need) return fail(ctx, OIDT_ERR_INVALID, "output needs %zu doubles", need);
+  if (need * 8 > kStaticScratchBytes)
+    return fail(ctx, OIDT_ERR_INVALID,
+                "the DFT window needs %zu bytes of device scratch; the static scratch holds %zu (use oidt_job_read_dft)",
+                need * 8, kStaticScratchBytes);
+  if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, OIDT_ERR_INVALID, "device ordinal out of range");
+  int rc = read_common(ctx, J);
+  if (rc) return rc;
+  void *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> gs(g_static_mu);
+    if (!g_static_addr[ctx->device]) {
+      void *a = nullptr;
+      CU(ctx, cudaGetSymbolAddress(&a, g_static_scratch));
+      g_static_addr[ctx->device] = a;
+    }
+    scratch = g_static_addr[ctx->device];
+  }
+  const double2 *acc = reinterpret_cast<const double2 *>(J->mem + J->pl.off_acc) + ((size_t)port * nc + comp) * J->d.nf * J->pl.plane;
+  const long long blocks = std::min<long long>((long long)(cells + 255) / 256, 148LL * 8);
+  k_gather_window<<<(unsigned)std::max(1LL, blocks), 256, 0, ctx->stream>>>(
+      acc, static_cast<double2 *>(scratch), J->d.nf, J->pl.plane, is3 ? J->d.ny : 0, i0, wi, j0, wj);
+  CU(ctx, cudaGetLastError());
+  ctx->launches += 1;
+  CU(ctx, cudaMemcpyAsync(out, scratch, need * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CU(ctx, cudaStreamSynchronize(ctx->stream));
+  return OIDT_OK;
+}
+
 static bool field_ok(Job *J, int field) {
   if (field < 0 || field > 5) return false;
   std::vector<int> f = fields_of(J->d.mode);

@@ -21,7 +21,8 @@ OK, ERR_INVALID, ERR_CUDA, ERR_BUDGET, ERR_NOTFOUND, ERR_TIMEOUT, ERR_STATE = 0,
 EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error", "oidt_stats_get",
            "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
            "oidt_job_query", "oidt_job_read_dft", "oidt_job_read_field", "oidt_job_write_field",
-           "oidt_job_read_psi", "oidt_job_release", "oidt_job_reset", "oidt_ctx_stream", "oidt_job_profile")
+           "oidt_job_read_psi", "oidt_job_release", "oidt_job_reset", "oidt_ctx_stream", "oidt_job_profile",
+           "oidt_job_read_dft_window_static")
 
 
 class OidtError(RuntimeError):
@@ -70,6 +71,7 @@ def load_library(path: str = LIB_PATH):
             "oidt_job_sync": ([vp, u64, i32], i32),
             "oidt_job_query": ([vp, u64, C.POINTER(i32), C.POINTER(i32)], i32),
             "oidt_job_read_dft": ([vp, u64, i32, i32, vp, C.c_size_t], i32),
+            "oidt_job_read_dft_window_static": ([vp, u64, i32, i32, vp, C.c_size_t], i32),
             "oidt_job_read_field": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_write_field": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_read_psi": ([vp, u64, i32, i32, i32, vp, C.c_size_t], i32),
@@ -185,6 +187,19 @@ class Job:
         out = np.empty((self.spec.nf,) + tuple(plane), dtype=np.complex128)
         self.eng._check(self.eng.lib.oidt_job_read_dft(self.eng.ctx, self.id, port, ci,
                                                        out.ctypes.data, out.size * 2))
+        return out
+
+    def dft_window_static(self, port: int, comp) -> np.ndarray:
+        """complex128 DFT of one port component over the DFT window only
+        ([nf][wi][wj] in 3D, [nf][wj] in 2D), read through the entry point
+        that allocates no device memory."""
+        comps = DFT_COMPS[self.spec.mode]
+        ci = comps.index(comp) if isinstance(comp, str) else comp
+        (i0, j0), (i1, j1) = self.spec.win_lo, self.spec.win_hi
+        win = (i1 - i0, j1 - j0) if self.spec.mode == "yee3d" else (j1 - j0,)
+        out = np.empty((self.spec.nf,) + win, dtype=np.complex128)
+        self.eng._check(self.eng.lib.oidt_job_read_dft_window_static(self.eng.ctx, self.id, port, ci,
+                                                                     out.ctypes.data, out.size * 2))
         return out
 
     def field(self, name: str) -> np.ndarray:
