@@ -301,6 +301,13 @@ def run_engine(args, ws, rank, local):
     e2e = dist_max(dist, float(np.mean(e2e_ms)), local)
     e2e_value = ws * spec.ncells * spec.nt / (e2e * 1e-3) / 1e9
 
+    # ---- batched realizations and the served mix (rank 0) ----------------
+    batched = serving = None
+    if rank == 0 and not args.no_extra:
+        from oidt_b200 import batch as B, serve as SV
+        batched = B.measure(eng, n=args.batch_n, steps=3000)
+        serving = SV.measure(eng, rate_hz=20.0, duration_s=args.serve_window)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline(spec, target_s=args.cpu_seconds)
@@ -326,6 +333,8 @@ def run_engine(args, ws, rank, local):
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e, 3)},
             "gpu_launches": int(launches),
+            "batched": batched,
+            "serving": serving,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -342,6 +351,9 @@ def main():
     ap.add_argument("--impl", default="engine", choices=("engine", "reference"))
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched-realization and served-mix measurements")
+    ap.add_argument("--batch-n", type=int, default=16, help="realizations in the batched-vs-plain measurement")
+    ap.add_argument("--serve-window", type=float, default=3.0, help="seconds of served-mix arrivals (20 jobs/s)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":

@@ -77,3 +77,23 @@ def run_plain(eng: Engine, specs, precision=np.float32):
 def s21_loss_db(results, freqs=None):
     """Per-realization insertion loss -20 log10 |S21| averaged over the band."""
     return np.array([float(np.mean(-20 * np.log10(np.abs(r["S21"])))) for r in results])
+
+
+def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0):
+    """Realizations/s of the batched path against the plain one-run-at-a-time
+    path on ``n`` realizations drawn like the batched stochastic set (uneven
+    grids), plus the largest |S21 difference| between the two (the same
+    arithmetic, so 0 is expected).  Each realization is a rough run and the
+    smooth incident run of its grid."""
+    specs = realization_specs(W.batch_configs(n=n, master_seed=master_seed, steps=steps), nf=nf)
+    cells = sum(r.ncells * r.nt + i.ncells * i.nt for r, i in specs)
+    t_plain, s_plain = run_plain(eng, specs)
+    t_batch, s_batch = run_batched(eng, specs)
+    d = max(float(np.max(np.abs(a["S21"] - b["S21"]))) for a, b in zip(s_plain, s_batch))
+    return {"realizations": n, "steps": steps, "nf": nf, "cell_updates": int(cells),
+            "plain_s": round(t_plain, 3), "batched_s": round(t_batch, 3),
+            "plain_realizations_per_s": round(n / t_plain, 3), "batched_realizations_per_s": round(n / t_batch, 3),
+            "speedup": round(t_plain / t_batch, 3), "max_abs_dS21_batched_vs_plain": d,
+            "s21_loss_db_mean": float(np.mean(s21_loss_db(s_batch))),
+            "s21_loss_db_std": float(np.std(s21_loss_db(s_batch)))}
+

@@ -22,6 +22,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import workloads as W
 from .engine import BudgetError, Engine
 from .sparams import forward_s
 
@@ -144,3 +145,41 @@ def latency_stats(results):
     lat = np.array([r.latency for r in results]) if results else np.zeros(1)
     return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "n": len(results)}
+
+
+def requests_from_mix(mix, nf=21, precision=np.float32):
+    """Requests for a served mix (``workloads.serving_mix``): each is a rough
+    run with the smooth incident run of the same grid (S21 needs both)."""
+    out = []
+    for rid, (t, kw) in enumerate(mix):
+        kw = dict(kw)
+        kind = kw.pop("kind")
+        if kind == "2d":
+            nx = kw["nx"]
+            common = dict(nx=nx, ny=kw["ny"], P=10, core_cells=10, src_x=40, ports=(60, nx - 60), steps=kw["steps"],
+                          nf=nf, precision=precision, sigma_nm=kw["sigma_nm"], lc_nm=kw["lc_nm"], seed=kw["seed"])
+            spec, inc = W.slab2d(rough=True, **common), W.slab2d(rough=False, **common)
+        else:
+            common = dict(nx=kw["nx"], ny=kw["ny"], nz=kw["nz"], P=10, steps=kw["steps"], nf=nf, precision=precision,
+                          sigma_nm=kw["sigma_nm"], lc_nm=kw["lc_nm"], seed=kw["seed"])
+            spec, inc = W.strip3d(rough=True, **common), W.strip3d(rough=False, **common)
+        out.append(Request(rid, t, spec, incident=inc, meta={"kind": kind}))
+    return out
+
+
+def measure(eng: Engine, rate_hz=20.0, duration_s=3.0, seed=0, tick=64, max_wall=300.0):
+    """Serve the first ``duration_s`` seconds of the served mix at ``rate_hz``
+    with arrivals honoured on the wall clock; latency and throughput."""
+    reqs = requests_from_mix(W.serving_mix(rate_hz=rate_hz, duration_s=duration_s, seed=seed))
+    srv = Server(eng, tick=tick)
+    t0 = time.perf_counter()
+    res = srv.run(reqs, realtime=True, max_wall=max_wall)
+    wall = time.perf_counter() - t0
+    cells = sum(r.cells * r.steps for r in res) + sum(q.incident.ncells * q.incident.nt for q in reqs
+                                                        if q.rid in {r.rid for r in res})
+    st = latency_stats(res)
+    return {"rate_hz": rate_hz, "arrival_window_s": duration_s, "requests": len(reqs), "completed": len(res),
+            "p50_s": round(st["p50_s"], 3), "p99_s": round(st["p99_s"], 3), "mean_s": round(st["mean_s"], 3),
+            "wall_s": round(wall, 3), "jobs_per_s": round(len(res) / wall, 3),
+            "gcell_updates_per_s": round(cells / wall / 1e9, 3), "admission_refusals": srv.refused}
+

@@ -270,8 +270,12 @@ def cases(ref):
                 usr = pickle.load(open(os.path.join(ref, SOLVER_DIR[mode], "user_dict.pkl"), "rb"))
                 usr = dict(usr, precision=prec, sparam_num_freqs=7, rough_toggle=False, feedback_at_n_percent=50)
                 if mode == "yee3d":
-                    usr.update(num_lines=1, sgl_wg_length=1.0e-6, port1_length=0.25e-6, port2_length=0.25e-6,
-                               nx_clad_wl=0.5, ny_clad_wl=0.5)
+                    # pitch 0.4 um: the reference's auto-setup requires a cladding buffer of at least
+                    # half the waveguide pitch (fdtd_auto_setup.py:121-122); port lengths whose cell
+                    # counts carry when summed: its incident runs set the guide length to
+                    # port1 + port2 and require p2z > p1z (fdtd_auto_setup.py:88-89, 168-171)
+                    usr.update(num_lines=1, sgl_wg_length=1.0e-6, port1_length=0.21e-6, port2_length=0.21e-6,
+                               nx_clad_wl=0.5, ny_clad_wl=0.5, pitch=0.4e-6)
                 run_case(ref, nm, mode, usr, [(0, "f", "r"), (0, "b", "i")], setup_only=True)
             c[nm] = mk
     return c
