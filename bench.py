@@ -43,24 +43,36 @@ def dist_env():
     return ws, rank, local
 
 
-def dist_init(ws, local):
+def dist_init(ws, local, backend="nccl"):
+    """Process group of the replica ranks (NCCL on the GPU box; gloo serves
+    the CPU tests of the same code).  A short timeout ends a rank that waits
+    for a lost peer with an error instead of a hang."""
     if ws <= 1:
         return None
     import datetime
     import torch
     import torch.distributed as dist
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return dist
 
 
 def dist_max(dist, x, local):
+    """Max over ranks (the slowest replica's time)."""
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
+    dev = "cuda:%d" % local if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(ws, cells_per_rank, steps, ms_max):
+    """Gcell-updates/s of all replicas: every rank advances its own grid, the
+    job takes as long as the slowest rank."""
+    return ws * cells_per_rank * steps / (ms_max * 1e-3) / 1e9
 
 
 def barrier(dist):
@@ -261,7 +273,7 @@ def run_engine(args, ws, rank, local):
     barrier(dist)
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = dist_max(dist, ms, local)
-    value = ws * spec.ncells * spec.nt / (ms * 1e-3) / 1e9
+    value = whole_job_rate(ws, spec.ncells, spec.nt, ms)
 
     # ---- per-kernel roofline (live CUDA events on the engine stream) -----
     # A time step is two launches, the E half-step (k_y3_e, the larger one)
@@ -299,7 +311,7 @@ def run_engine(args, ws, rank, local):
             e2e_ms.append((t1 - t0) * 1e3)
         del outs
     e2e = dist_max(dist, float(np.mean(e2e_ms)), local)
-    e2e_value = ws * spec.ncells * spec.nt / (e2e * 1e-3) / 1e9
+    e2e_value = whole_job_rate(ws, spec.ncells, spec.nt, e2e)
 
     # ---- batched realizations and the served mix (rank 0) ----------------
     batched = serving = None
