@@ -140,6 +140,14 @@ class Engine:
         del keep
         return Job(self, jid.value, spec, np.dtype(precision if precision is not None else spec.precision))
 
+    def mark(self):
+        """A marker of the work enqueued so far on the context's stream (a CUDA
+        event); ``.synchronize()`` waits for that work."""
+        import torch
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.ExternalStream(self.stream_handle(), device=self.device))
+        return ev
+
     def stream_handle(self) -> int:
         """The compute stream (cudaStream_t as an integer)."""
         h = C.c_void_p()

@@ -80,35 +80,57 @@ class Server:
         self.active.append((req, j, ji, now))
         return True
 
-    def _retire(self, t0: float):
-        keep = []
-        for (req, j, ji, adm) in self.active:
-            jobs = [x for x in (j, ji) if x is not None]
-            if all(x.steps >= x.spec.nt for x in jobs):
-                for x in jobs:
-                    x.sync()
-                nc = 4 if req.spec.mode == "yee3d" else 2
-                d_ref = {(p, c): j.dft(p, c) for p in (0, 1) for c in range(nc)}
-                d_inc = {(p, c): ji.dft(p, c) for p in (0, 1) for c in range(nc)} if ji is not None else d_ref
-                S = forward_s(req.spec, d_inc, d_ref)
-                fin = time.perf_counter() - t0
-                self.results.append(Result(req.rid, req.arrival, adm, fin, req.spec.ncells, req.spec.nt,
-                                           S={k: v for k, v in S.items() if k != "P_inc"},
-                                           dfts=d_ref if self.keep_dfts else None))
-                for x in jobs:
-                    x.release()
-            else:
-                keep.append((req, j, ji, adm))
-        self.active = keep
+    def _finish(self, entry, t0: float):
+        """Read the DFTs of a completed request, compute S, free its jobs."""
+        req, j, ji, adm = entry
+        jobs = [x for x in (j, ji) if x is not None]
+        for x in jobs:
+            x.sync()
+        nc = 4 if req.spec.mode == "yee3d" else 2
+        d_ref = {(p, c): j.dft(p, c) for p in (0, 1) for c in range(nc)}
+        d_inc = {(p, c): ji.dft(p, c) for p in (0, 1) for c in range(nc)} if ji is not None else d_ref
+        S = forward_s(req.spec, d_inc, d_ref)
+        fin = time.perf_counter() - t0
+        self.results.append(Result(req.rid, req.arrival, adm, fin, req.spec.ncells, req.spec.nt,
+                                   S={k: v for k, v in S.items() if k != "P_inc"},
+                                   dfts=d_ref if self.keep_dfts else None))
+        for x in jobs:
+            x.release()
 
-    def run(self, requests, realtime: bool = True, max_wall: float = None):
+    def _tick(self):
+        """Enqueue one tick for every admitted request with steps left; returns
+        the requests whose last steps are now enqueued."""
+        jobs = []
+        for (req, j, ji, adm) in self.active:
+            jobs += [x for x in (j, ji) if x is not None and x.steps < x.spec.nt]
+        left = [x.spec.nt - x.steps for x in jobs]
+        full = [x for x, l in zip(jobs, left) if l >= self.tick]
+        rest = [(x, l) for x, l in zip(jobs, left) if 0 < l < self.tick]
+        by_prec = {}
+        for x in full:
+            by_prec.setdefault(str(x.precision), []).append(x)
+        for group in by_prec.values():
+            self.eng.batch_advance(group, self.tick)
+        for x, l in rest:
+            x.advance(l)
+        done, keep = [], []
+        for e in self.active:
+            (done if all(x.steps >= x.spec.nt for x in e[1:3] if x is not None) else keep).append(e)
+        self.active = keep
+        return done
+
+    def run(self, requests, realtime: bool = True, max_wall: float = None, depth: int = 2):
         """Serve ``requests`` (sorted by arrival).  With ``realtime`` the
         arrival times are honoured against the wall clock; otherwise every
-        request is available immediately (throughput mode)."""
+        request is available immediately (throughput mode).  Up to ``depth``
+        ticks are in flight on the device while the host admits, reads out and
+        retires, so the device does not wait for host work."""
+        import collections
         pending = sorted(requests, key=lambda r: r.arrival)
+        inflight = collections.deque()  # (event, requests completed by that tick)
         t0 = time.perf_counter()
         qi = 0
-        while qi < len(pending) or self.active:
+        while qi < len(pending) or self.active or inflight:
             now = time.perf_counter() - t0
             if max_wall is not None and now > max_wall:
                 break
@@ -118,26 +140,21 @@ class Server:
                     self.refused += 1
                     break
                 qi += 1
-            if not self.active:
-                if qi < len(pending) and realtime:
-                    time.sleep(max(0.0, min(0.01, pending[qi].arrival - now)))
-                continue
-            jobs = []
-            for (req, j, ji, adm) in self.active:
-                jobs += [x for x in (j, ji) if x is not None]
-            left = [x.spec.nt - x.steps for x in jobs]
-            full = [x for x, l in zip(jobs, left) if l >= self.tick]
-            rest = [(x, l) for x, l in zip(jobs, left) if 0 < l < self.tick]
-            by_prec = {}
-            for x in full:
-                by_prec.setdefault((str(x.precision)), []).append(x)
-            for group in by_prec.values():
-                self.eng.batch_advance(group, self.tick)
-            for x, l in rest:
-                x.advance(l)
-            if jobs:
-                jobs[0].sync()  # one stream: waiting on any job waits for the tick
-            self._retire(t0)
+            launched = False
+            if self.active:
+                done = self._tick()
+                inflight.append((self.eng.mark(), done))
+                launched = True
+            # keep at most `depth` ticks queued; drain when there is nothing to launch
+            while inflight and (len(inflight) >= depth or not launched):
+                ev, done = inflight.popleft()
+                ev.synchronize()
+                for e in done:
+                    self._finish(e, t0)
+                if not launched:
+                    break
+            if not launched and not inflight and qi < len(pending) and realtime:
+                time.sleep(max(0.0, min(0.01, pending[qi].arrival - (time.perf_counter() - t0))))
         return self.results
 
 
