@@ -1,13 +1,18 @@
 """Batched stochastic-roughness realizations.
 
-Each realization is a rough 3D strip of its own (uneven) size plus the smooth
-incident run of the same grid; S21 = sqrt(P_port2(rough) / P_port1(smooth)).
+Each realization is a rough 3D strip of its own (uneven) size.  Its S21 is
+sqrt(P_port2(rough) / P_port1(incident)), where the incident run is a smooth
+guide just long enough for both ports -- the reference's incident runs shorten
+the guide to the two port lengths (FDTD_3D fdtd_auto_setup.py:88-89).  The
+incident run depends only on the cross-section, the time steps and the
+source, not on the roughness or the guide length, so:
 
-* :func:`run_batched` -- all realizations' runs advance together: one
-  plane-sweep launch per time step over every job's work items (per-job tile
-  tables), K-step blocks replayed from a CUDA graph.
-* :func:`run_plain` -- the same kernels one run at a time, no graph (the
-  baseline the batched rate is compared with).
+* :func:`run_plain` -- one run at a time, as the reference runs each line:
+  every realization runs its rough guide and its own incident run, each
+  launched step by step (no graph).
+* :func:`run_batched` -- every rough run plus one shared incident run per
+  cross-section advance together in multi-job launches (one branch per job,
+  K-step blocks replayed from a CUDA graph).
 """
 from __future__ import annotations
 
@@ -20,61 +25,73 @@ from .engine import Engine
 from .sparams import forward_s
 
 
-def realization_specs(configs, nf=41, precision=np.float32, **common):
-    out = []
+def incident_length(kw: dict) -> int:
+    """Cells along the guide of the incident run: the CPML, the source gap and
+    the port gap on both sides, plus two cells between the ports."""
+    P, src_gap, port_gap = kw.get("P", 10), kw.get("src_gap", 10), kw.get("port_gap", 20)
+    return 2 * (P + src_gap + port_gap) + 2
+
+
+def realization_set(configs, nf=41, precision=np.float32, **common):
+    """Rough specs, the incident key of each, and the incident specs by key
+    ((nx, ny, steps): realizations of one cross-section share one)."""
+    roughs, keys, incidents = [], [], {}
     for c in configs:
         kw = dict(nx=c["nx"], ny=c["ny"], nz=c["nz"], steps=c["steps"], nf=nf, sigma_nm=c["sigma_nm"],
                   lc_nm=c["lc_nm"], seed=c["seed"], precision=precision)
         kw.update(common)
-        out.append((W.strip3d(**kw), W.strip3d(rough=False, **kw)))
-    return out
+        roughs.append(W.strip3d(**kw))
+        key = (c["nx"], c["ny"], c["steps"])
+        if key not in incidents:
+            incidents[key] = W.strip3d(**dict(kw, rough=False, nz=incident_length(kw)))
+        keys.append(key)
+    return roughs, keys, incidents
 
 
-def _s21(spec_r, job_i, job_r):
-    inc = {(p, c): job_i.dft(p, c) for p in (0, 1) for c in range(4)}
-    ref = {(p, c): job_r.dft(p, c) for p in (0, 1) for c in range(4)}
-    return forward_s(spec_r, inc, ref)
+def _dfts(job):
+    return {(p, c): job.dft(p, c) for p in (0, 1) for c in range(4)}
 
 
-def run_batched(eng: Engine, specs, precision=np.float32, ring_steps=32, max_jobs=None):
-    """Advance every run of every realization in multi-job launches (in groups
-    of at most ``max_jobs`` jobs if given).  Returns (seconds, [S dict])."""
+def run_batched(eng: Engine, rset, precision=np.float32, ring_steps=32):
+    """Advance every rough run and the shared incident runs together.
+    Returns (seconds, [S dict per realization])."""
+    roughs, keys, incidents = rset
     t0 = time.perf_counter()
-    flat = [s for pair in specs for s in pair]
-    groups = [flat] if not max_jobs else [flat[i:i + max_jobs] for i in range(0, len(flat), max_jobs)]
-    res = []
-    for g in groups:
-        jobs = [eng.submit(s, precision=precision, ring_steps=ring_steps) for s in g]
-        steps = min(s.nt for s in g)
-        eng.batch_advance(jobs, steps)
-        for j in jobs:
-            if j.spec.nt > steps:
-                j.advance(j.spec.nt - steps)
-        for j in jobs:
-            j.sync()
-        for k in range(0, len(jobs), 2):
-            res.append(_s21(g[k], jobs[k + 1], jobs[k]))
-        for j in jobs:
-            j.release()
+    inc_keys = list(incidents)
+    specs = roughs + [incidents[k] for k in inc_keys]
+    jobs = [eng.submit(s, precision=precision, ring_steps=ring_steps) for s in specs]
+    steps = min(s.nt for s in specs)
+    eng.batch_advance(jobs, steps)
+    for j in jobs:
+        if j.spec.nt > steps:
+            j.advance(j.spec.nt - steps)
+    for j in jobs:
+        j.sync()
+    inc = {k: _dfts(jobs[len(roughs) + n]) for n, k in enumerate(inc_keys)}
+    res = [forward_s(roughs[r], inc[keys[r]], _dfts(jobs[r])) for r in range(len(roughs))]
+    for j in jobs:
+        j.release()
     return time.perf_counter() - t0, res
 
 
-def run_plain(eng: Engine, specs, precision=np.float32):
-    """One run at a time, no graph replay."""
+def run_plain(eng: Engine, rset, precision=np.float32):
+    """One run at a time, launched step by step: each realization's rough
+    run, then its own incident run."""
+    roughs, keys, incidents = rset
     t0 = time.perf_counter()
     res = []
-    for (sr, si) in specs:
-        jr = eng.submit(sr, precision=precision, graphs=False)
+    for spec_r, key in zip(roughs, keys):
+        jr = eng.submit(spec_r, precision=precision, graphs=False)
         jr.run().sync()
-        ji = eng.submit(si, precision=precision, graphs=False)
+        ji = eng.submit(incidents[key], precision=precision, graphs=False)
         ji.run().sync()
-        res.append(_s21(sr, ji, jr))
+        res.append(forward_s(spec_r, _dfts(ji), _dfts(jr)))
         jr.release()
         ji.release()
     return time.perf_counter() - t0, res
 
 
-def s21_loss_db(results, freqs=None):
+def s21_loss_db(results):
     """Per-realization insertion loss -20 log10 |S21| averaged over the band."""
     return np.array([float(np.mean(-20 * np.log10(np.abs(r["S21"])))) for r in results])
 
@@ -82,18 +99,19 @@ def s21_loss_db(results, freqs=None):
 def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0):
     """Realizations/s of the batched path against the plain one-run-at-a-time
     path on ``n`` realizations drawn like the batched stochastic set (uneven
-    grids), plus the largest |S21 difference| between the two (the same
-    arithmetic, so 0 is expected).  Each realization is a rough run and the
-    smooth incident run of its grid."""
-    specs = realization_specs(W.batch_configs(n=n, master_seed=master_seed, steps=steps), nf=nf)
-    cells = sum(r.ncells * r.nt + i.ncells * i.nt for r, i in specs)
-    t_plain, s_plain = run_plain(eng, specs)
-    t_batch, s_batch = run_batched(eng, specs)
+    grids), and the largest |S21 difference| between the two (the same
+    arithmetic on the same runs, so 0 is expected)."""
+    rset = realization_set(W.batch_configs(n=n, master_seed=master_seed, steps=steps), nf=nf)
+    roughs, keys, incidents = rset
+    plain_cells = sum(r.ncells * r.nt + incidents[k].ncells * incidents[k].nt for r, k in zip(roughs, keys))
+    batched_cells = sum(r.ncells * r.nt for r in roughs) + sum(s.ncells * s.nt for s in incidents.values())
+    t_plain, s_plain = run_plain(eng, rset)
+    t_batch, s_batch = run_batched(eng, rset)
     d = max(float(np.max(np.abs(a["S21"] - b["S21"]))) for a, b in zip(s_plain, s_batch))
-    return {"realizations": n, "steps": steps, "nf": nf, "cell_updates": int(cells),
+    loss = s21_loss_db(s_batch)
+    return {"realizations": n, "steps": steps, "nf": nf, "shared_incident_runs": len(incidents),
+            "plain_cell_updates": int(plain_cells), "batched_cell_updates": int(batched_cells),
             "plain_s": round(t_plain, 3), "batched_s": round(t_batch, 3),
             "plain_realizations_per_s": round(n / t_plain, 3), "batched_realizations_per_s": round(n / t_batch, 3),
             "speedup": round(t_plain / t_batch, 3), "max_abs_dS21_batched_vs_plain": d,
-            "s21_loss_db_mean": float(np.mean(s21_loss_db(s_batch))),
-            "s21_loss_db_std": float(np.std(s21_loss_db(s_batch)))}
-
+            "s21_loss_db_mean": float(np.mean(loss)), "s21_loss_db_std": float(np.std(loss))}
