@@ -156,7 +156,9 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_e(Params<T>
 }
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_h(Params<T> p, int s) {
-  const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = blockIdx.z;
+  // planes in decreasing i: the H half starts on the E planes the E half wrote
+  // last (still in L2), and ends on the planes the next E half reads first
+  const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = gridDim.z - 1 - blockIdx.z;
   const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
   if (!block_meets_src(p, i, j0, k0)) {
     // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
@@ -252,7 +254,8 @@ __global__ void __launch_bounds__(128) k_2d_e(Params<T> p, int s) {
 }
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128) k_2d_h(Params<T> p, int s) {
-  const int j = blockIdx.x * kBlock2 + threadIdx.x, i = blockIdx.y;
+  // rows in decreasing i (the E half's last rows are still in L2)
+  const int j = blockIdx.x * kBlock2 + threadIdx.x, i = gridDim.y - 1 - blockIdx.y;
   if (j >= p.ny) return;
   if (p.mode == OIDT_MODE_TM2)
     tm2_h_cell<T, EXACT>(p, i, j, p.state[0] + s, s);
