@@ -1118,6 +1118,37 @@ int set_sweep_attrs() {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+// ---- capture ring refill after a field write ----------------------------------
+// The update kernels write a component's sample into the capture ring only
+// where they update it; cells a step never updates (the PEC rim) keep their
+// value for the whole run, and the fold's colocation reaches them when the DFT
+// window touches the rim (a one-cell CPML).  After fields are written, every
+// ring slot is filled with the current port-plane values, so the slots no
+// update overwrites hold those constant values.  Slots: 3D Ex, Ey, Hx(k),
+// Hx(k+1), Hy(k), Hy(k+1) on the z = port planes; TM2 Ez, Hy(x), Hy(x+1) and
+// TE2 Ey, Hz(x), Hz(x+1) on the x = port planes.
+namespace {
+template <typename T> __global__ void k_ring_fill(Params<T> p) {
+  const long long n = (long long)p.ring_K * 2 * p.nslot * p.plane;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long c = t % p.plane, r = t / p.plane;
+    const int slot = (int)(r % p.nslot), q = (int)((r / p.nslot) % 2);
+    const int port = p.port_pos[q];
+    T v;
+    if (p.mode == OIDT_MODE_YEE3D) {
+      const int f = slot == 0 ? EX : slot == 1 ? EY : slot < 4 ? HX : HY;
+      const int d = (slot == 3 || slot == 5) ? 1 : 0;
+      v = p.f[f][c * p.nzp + port + d];
+    } else {
+      const int f = slot == 0 ? (p.mode == OIDT_MODE_TM2 ? EZ : EY) : (p.mode == OIDT_MODE_TM2 ? HY : HZ);
+      const int d = slot == 2 ? 1 : 0;
+      v = p.f[f][(long long)(port + d) * p.ny + c];
+    }
+    p.ring[t] = v;
+  }
+}
+}  // namespace
+
 extern "C" {
 
 int32_t oidt_abi_version(void) { return OIDT_ABI_VERSION; }
@@ -1432,6 +1463,14 @@ int32_t oidt_job_write_field(oidt_ctx *ctx, uint64_t job, int32_t field, const v
     rc = copy_grid_h2d(ctx, J, J->mem + J->pl.off_f[b][field], src, ctx->upload);
     if (rc) return rc;
   }
+  const long long n = (long long)J->pl.K * 2 * nslot_of(J->d.mode) * J->pl.plane;
+  const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 8);
+  if (J->d.precision == OIDT_F64)
+    k_ring_fill<double><<<blocks, 256, 0, ctx->upload>>>(cells<double>(J)[J->parity]);
+  else
+    k_ring_fill<float><<<blocks, 256, 0, ctx->upload>>>(cells<float>(J)[J->parity]);
+  CU(ctx, cudaGetLastError());
+  ctx->launches += 1;
   CU(ctx, cudaStreamSynchronize(ctx->upload));
   return OIDT_OK;
 }

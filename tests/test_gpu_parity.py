@@ -81,6 +81,14 @@ def _random_cases():
         # no CPML, edge or source cells (and a port plane inside one of them)
         "yee3d_wide": lambda: W.strip3d(nx=30, ny=44, nz=130, P=4, src_gap=2, port_gap=26, steps=40, nf=3,
                                         core_x_nm=160, core_y_nm=240, sigma_nm=20, lc_nm=60, seed=7),
+        # the thinnest CPML: P = 1 (no H-slab cells) and P = 2; the DFT window then reaches the
+        # rim cells no step updates
+        "yee3d_p1": lambda: W.strip3d(nx=16, ny=15, nz=29, P=1, src_gap=2, port_gap=3, steps=40, nf=3,
+                                      core_x_nm=100, core_y_nm=120, seed=8),
+        "yee3d_p2": lambda: W.strip3d(nx=17, ny=18, nz=35, P=2, src_gap=2, port_gap=4, steps=40, nf=3,
+                                      core_x_nm=100, core_y_nm=140, source="TM", seed=9),
+        "tm2_p1": lambda: W.slab2d(nx=40, ny=31, P=1, core_cells=7, src_x=6, ports=(10, 30), steps=40, nf=4,
+                                   rough=True, sigma_nm=30, lc_nm=60, seed=4),
     }
 
 
@@ -101,7 +109,8 @@ def _te2_spec():
 
 
 @pytest.mark.parametrize("name", ["tm2", "te2", "yee3d_te", "yee3d_tm", "yee3d_wide", "yee3d_te_cell",
-                                  "yee3d_tm_cell", "yee3d_wide_cell"])
+                                  "yee3d_tm_cell", "yee3d_wide_cell", "yee3d_p1", "yee3d_p1_cell",
+                                  "yee3d_p2", "yee3d_p2_cell", "tm2_p1"])
 @pytest.mark.parametrize("ring", [1, 7, 32])
 def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     variant = "cell" if name.endswith("_cell") else "sweep"
