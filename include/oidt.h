@@ -153,13 +153,19 @@ int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t com
 /* Port-window DFT of one (port, comp), as oidt_job_read_dft but restricted
  * to the DFT window [win_lo, win_hi): out = complex128 [nf][wi][wj] (3D, wi =
  * win_hi[0] - win_lo[0], wj = win_hi[1] - win_lo[1]) or [nf][wj] (2D),
- * interleaved re/im, n = number of doubles.  Allocates nothing: it stages
- * through a fixed 16 MiB static device buffer (larger windows are rejected
- * with OIDT_ERR_INVALID), for callers whose call path may not allocate
- * device memory.  The first call on a device resolves the buffer's address
- * (cudaGetSymbolAddress, which may load the module) and should come before
- * any stream capture on that device.  The buffer is shared by all contexts
- * on a device: calls on one device must not overlap.  No counterpart in the
+ * interleaved re/im, n = number of doubles.  Allocates nothing, for hosts
+ * that may not allocate device memory where they read results: a host that
+ * reserves its whole device budget at start-up (a fixed-budget serving
+ * process) or reads results from a callback where an allocation could
+ * block on, or fail under, memory held by others.  It stages through a fixed
+ * 16 MiB static device buffer, held on every GPU that loads the library
+ * until the process exits; windows needing more are rejected with
+ * OIDT_ERR_INVALID.  Nothing in the buffer has to start at zero: every
+ * element read was written by the same call.  The first call on a device
+ * resolves the buffer's address (cudaGetSymbolAddress, which may load the
+ * module) and should come before any stream capture on that device.  All
+ * contexts on a device share the buffer, which keeps the last call's
+ * contents: calls that overlap on one device race.  No counterpart in the
  * reference (its DFT arrays come back whole, fdtd_main.py:349-386). */
 int32_t oidt_job_read_dft_window_static(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t comp,
                                         double *out, size_t n);

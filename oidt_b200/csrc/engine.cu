@@ -1370,7 +1370,7 @@ int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t com
 // serialised by its mutex).
 namespace {
 constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB: 1 Mi complex doubles
-__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 std::mutex g_static_mu;
 constexpr int kMaxDevices = 64;
 void *g_static_addr[kMaxDevices] = {};  // resolved once per device

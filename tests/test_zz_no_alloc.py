@@ -1,8 +1,10 @@
-"""The allocation-free port-window DFT readout (oidt_job_read_dft_window_static)
-equals the window of the staged full-plane readout (oidt_job_read_dft), on two
-consecutive calls and for 2D and 3D jobs; windows larger than its static
-device scratch are refused.  Collected last so it also runs after the rest of
-the suite on the same device."""
+"""The allocation-free port-window DFT readout (oidt_job_read_dft_window_static),
+meant for hosts that reserve their device memory up front and may not allocate
+when they read results, equals the window of the staged full-plane readout
+(oidt_job_read_dft), bit for bit, on two consecutive calls and for 2D and 3D
+jobs; windows larger than its 16 MiB static device buffer are refused.
+Collected last, so a run that stops at the first failure has already run
+every other test; it passes alone and after the rest of the suite."""
 import numpy as np
 import pytest
 
