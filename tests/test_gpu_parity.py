@@ -89,7 +89,18 @@ def _random_cases():
                                       core_x_nm=100, core_y_nm=140, source="TM", seed=9),
         "tm2_p1": lambda: W.slab2d(nx=40, ny=31, P=1, core_cells=7, src_x=6, ports=(10, 30), steps=40, nf=4,
                                    rough=True, sigma_nm=30, lc_nm=60, seed=4),
+        # dt/eps coefficient grids perturbed cell by cell (thousands of distinct (x, y, z) triples),
+        # so no cell's update can lean on a neighbour's coefficients
+        "yee3d_graded": lambda: _graded(W.strip3d(nx=22, ny=19, nz=37, P=4, src_gap=2, port_gap=3, steps=40,
+                                                  nf=4, core_x_nm=120, core_y_nm=160, seed=10)),
     }
+
+
+def _graded(spec):
+    rng = np.random.default_rng(11)
+    for k in spec.cb:
+        spec.cb[k] = spec.cb[k] * (1.0 + 0.01 * rng.random(spec.cb[k].shape))
+    return spec
 
 
 def _te2_spec():
@@ -110,7 +121,7 @@ def _te2_spec():
 
 @pytest.mark.parametrize("name", ["tm2", "te2", "yee3d_te", "yee3d_tm", "yee3d_wide", "yee3d_te_cell",
                                   "yee3d_tm_cell", "yee3d_wide_cell", "yee3d_p1", "yee3d_p1_cell",
-                                  "yee3d_p2", "yee3d_p2_cell", "tm2_p1"])
+                                  "yee3d_p2", "yee3d_p2_cell", "tm2_p1", "yee3d_graded", "yee3d_graded_cell"])
 @pytest.mark.parametrize("ring", [1, 7, 32])
 def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     variant = "cell" if name.endswith("_cell") else "sweep"
