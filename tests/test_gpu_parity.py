@@ -33,7 +33,8 @@ def eng():
 
 def _fixture_cases():
     out = []
-    for case in ["tm2_smooth", "tm2_rough2", "te2_smooth", "te2_rough2", "yee3d_smooth", "yee3d_rough2_tm"]:
+    for case in ["tm2_smooth", "tm2_rough2", "tm2_lines2", "te2_smooth", "te2_rough2", "yee3d_smooth",
+                 "yee3d_rough2_tm"]:
         if os.path.exists(os.path.join(G.GOLDEN, case + ".npz")):
             out.append(case)
     return out
@@ -265,3 +266,24 @@ def test_reset_reruns_identically(eng):
         np.testing.assert_array_equal(arr, first[f])
     np.testing.assert_array_equal(job.dft(1, 3), d1)
     job.release()
+
+
+@pytest.mark.parametrize("batch", [False, True])
+def test_two_line_launcher_equals_reference_smatrix(tmp_path, batch):
+    """The launcher's 8 runs of two coupled lines (one at a time, or all 8
+    advanced together) give the reference's 4 x 4 S-matrix bit for bit
+    (float64, exact arithmetic), and a touchstone file of 4 ports."""
+    from oidt_b200.simulation_launcher import launch
+    from oidt_b200.sparams import extract_sparams, read_touchstone
+    z = G.load("tm2_lines2")
+    usr = G.usr_of(z)
+    path = launch(usr, "tm2", cwd=str(tmp_path), batch=batch, verbose=False)
+    assert path.endswith(".s4p")
+    out = os.path.join(str(tmp_path), usr["output_dir"])
+    data = {f[:-4]: np.load(os.path.join(out, f)) for f in os.listdir(out) if f.endswith(".npy")}
+    assert len(data) == 24  # per line: fi, bi, ft, br, fr, bt, each Ez and Hy, as the reference saves
+    S = extract_sparams(usr, "tm2", data)
+    np.testing.assert_array_equal(S, z["S_mat"])
+    freqs, S_file, _ = read_touchstone(path)
+    assert S_file.shape == S.shape
+

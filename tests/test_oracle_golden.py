@@ -13,7 +13,7 @@ import pytest
 from oracle import fdtd_ref as R
 from tests import golden_io as G
 
-RUN_CASES = ["tm2_smooth", "tm2_rough2", "te2_smooth", "te2_rough2", "yee3d_smooth", "yee3d_rough2_tm"]
+RUN_CASES = ["tm2_smooth", "tm2_rough2", "tm2_lines2", "te2_smooth", "te2_rough2", "yee3d_smooth", "yee3d_rough2_tm"]
 SETUP_CASES = ["setup_%s_%s" % (m, p) for m in ("tm2", "te2", "yee3d") for p in ("float32", "float64")]
 
 

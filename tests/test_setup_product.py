@@ -12,7 +12,7 @@ from oracle import fdtd_ref as R
 from tests import golden_io as G
 
 SETUP_CASES = ["setup_%s_%s" % (m, p) for m in ("tm2", "te2", "yee3d") for p in ("float32", "float64")]
-RUN_CASES = ["tm2_smooth", "tm2_rough2", "te2_smooth", "te2_rough2", "yee3d_smooth", "yee3d_rough2_tm"]
+RUN_CASES = ["tm2_smooth", "tm2_rough2", "tm2_lines2", "te2_smooth", "te2_rough2", "yee3d_smooth", "yee3d_rough2_tm"]
 
 
 def spec_array(spec, name):
@@ -95,7 +95,7 @@ def test_product_setup_matches_oracle(case):
         assert tuple(spec.port_pos) == pp
 
 
-@pytest.mark.parametrize("case", [c for c in RUN_CASES if c.endswith("smooth")])
+@pytest.mark.parametrize("case", [c for c in RUN_CASES if c.endswith("smooth") or c == "tm2_lines2"])
 def test_product_extraction_matches_reference(case):
     """oidt_b200.sparams.extract_sparams on the reference's own saved .npy
     DFTs equals the S-matrix the reference's extract_sparams.py built."""
