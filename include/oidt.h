@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define OIDT_ABI_VERSION 1
+#define OIDT_ABI_VERSION 2  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe) */
 
 /* status codes */
 #define OIDT_OK 0
@@ -102,7 +102,14 @@ typedef struct oidt_job_desc {
    *              1 = plane sweep (one launch per step);
    * reserved[1]: 1 = launch every step directly (no CUDA-graph replay);
    * others must be 0. */
-  int32_t reserved[7];
+  int32_t reserved[4];
+  /* 3D time-domain line probe, the wave-impedance runs' recording
+   * (FDTD/GPU/FDTD_3D/wave_impedance/fdtd_main.py:298-299, fdtd_funcs.py:
+   * map_efield_zwave / map_hfield_zwave): probe[0] = 1 records after every
+   * step, for x in [0, ie), Ey(x, y, z) averaged over y, y+1; Ez averaged over
+   * z, z+1; Hy over (x, x+1) x (z, z+1); Hz over (x, x+1) x (y, y+1), at
+   * y = probe[1], z = probe[2].  probe[0] = 0: no probe (probe[1..2] 0). */
+  int32_t probe[3];
 } oidt_job_desc;
 
 typedef struct oidt_stats {
@@ -150,6 +157,13 @@ int32_t oidt_job_query(oidt_ctx *ctx, uint64_t job, int32_t *steps_done, int32_t
 int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t comp,
                           double *out_re_im, size_t n_doubles);
 
+/* Line-probe record of one component as [nt][nx] elements of the job's
+ * precision (rows of steps not yet run are 0).  comp: 0 = Ey, 1 = Ez,
+ * 2 = Hy, 3 = Hz.  Replaces the wave-impedance runs' copy of their
+ * [nt, nx] recordings (FDTD/GPU/FDTD_3D/wave_impedance/fdtd_main.py:341-346).
+ * OIDT_ERR_STATE if the job has no probe. */
+int32_t oidt_job_read_probe(oidt_ctx *ctx, uint64_t job, int32_t comp, void *out, size_t nbytes);
+
 /* Port-window DFT of one (port, comp), as oidt_job_read_dft but restricted
  * to the DFT window [win_lo, win_hi): out = complex128 [nf][wi][wj] (3D, wi =
  * win_hi[0] - win_lo[0], wj = win_hi[1] - win_lo[1]) or [nf][wj] (2D),
@@ -195,7 +209,7 @@ int32_t oidt_ctx_stream(oidt_ctx *ctx, void **stream);
  * events on the compute stream; ms_out[0..2] receive the average duration of
  * the E-half, H-half and DFT-fold launches.  Replaces the reference's
  * wall-clock MCells/s print (fdtd_main.py:306-341) with per-kernel device
- * times. */
+ * times.  A line probe records these steps too (its launches are not timed). */
 int32_t oidt_job_profile(oidt_ctx *ctx, uint64_t job, int32_t nsteps, float *ms_out);
 
 #ifdef __cplusplus

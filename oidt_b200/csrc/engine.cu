@@ -49,6 +49,36 @@ constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread
 constexpr int kVariantCell = 0, kVariantSweep = 1;  // oidt_job_desc.reserved[0]
 
 // ---------------------------------------------------------------------------
+// Line probe (wave-impedance recording): after every step, colocated Ey, Ez,
+// Hy, Hz along x at (y, z) = (jc, kc) into out[comp][n][x], x in [0, ie)
+// (FDTD/GPU/FDTD_3D/wave_impedance/fdtd_funcs.py map_efield_zwave /
+// map_hfield_zwave: 0.5 (a + b) and 0.25 (a + b + c + d) in that order).
+// ---------------------------------------------------------------------------
+template <typename T> struct ProbeArgs {
+  const T *ey, *ez, *hy, *hz;  // fields holding the state after the step
+  T *out;                      // [4][nt][nx]
+  int nx, nt, ie, jc, kc;
+  long long sy, sx;            // row and plane strides (elements)
+  const int *state;            // state[0] = absolute step of ring slot 0
+};
+
+template <typename T, bool EXACT> __global__ void __launch_bounds__(128) k_probe(ProbeArgs<T> a, int s) {
+  using A = Ar<T, EXACT>;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.state[0] + s;
+  if (x >= a.ie || n >= a.nt) return;
+  const long long c = x * a.sx + a.jc * a.sy + a.kc;  // (x, jc, kc)
+  const T half = T(0.5), quarter = T(0.25);
+  const size_t row = (size_t)n * a.nx + x, comp = (size_t)a.nt * a.nx;
+  a.out[row] = A::mul(half, A::add(a.ey[c], a.ey[c + a.sy]));
+  a.out[comp + row] = A::mul(half, A::add(a.ez[c], a.ez[c + 1]));
+  a.out[2 * comp + row] =
+      A::mul(quarter, A::add(A::add(A::add(a.hy[c], a.hy[c + a.sx]), a.hy[c + 1]), a.hy[c + a.sx + 1]));
+  a.out[3 * comp + row] =
+      A::mul(quarter, A::add(A::add(A::add(a.hz[c], a.hz[c + a.sx]), a.hz[c + a.sy]), a.hz[c + a.sx + a.sy]));
+}
+
+// ---------------------------------------------------------------------------
 // Per-cell launches (2D, and the 3D per-cell variant): in place.
 // ---------------------------------------------------------------------------
 // A block of the 3D per-cell launches covers kBlock3Z (k) x kBlock3Y (j) cells
@@ -425,6 +455,7 @@ struct JobPlan {
   size_t off_f[2][6], off_cb[3], off_kd[6], off_rkd[6], off_be, off_ce, off_bh, off_ch;
   size_t off_psi[2][6][3][2];
   size_t off_jsrc, off_tw[4], off_ring, off_acc, off_state, off_tmaps, off_items;
+  size_t off_probe, probe_bytes;  // line probe [4][nt][nx] (probe_bytes = 0: none)
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
 };
@@ -545,6 +576,13 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
         (long long)d->nx * d->ny * P > lim)
       return bad("grid too large: an x-plane or a CPML slab holds 2^31 or more elements");
   }
+  if (d->probe[0] != 0) {
+    if (d->probe[0] != 1 || !is3) return bad("probe[0] must be 0, or 1 (3D line probe)");
+    if (d->probe[1] < 0 || d->probe[1] + 1 >= d->ny || d->probe[2] < 0 || d->probe[2] + 1 >= d->nz)
+      return bad("line probe needs 0 <= y < ny - 1 and 0 <= z < nz - 1");
+  } else if (d->probe[1] != 0 || d->probe[2] != 0) {
+    return bad("probe[1..2] must be 0 without a probe");
+  }
   const int variant = is3 && d->reserved[0] == kVariantSweep ? kVariantSweep : kVariantCell;
   const int esz = d->precision == OIDT_F32 ? 4 : 8;
   const int nzp = is3 ? (int)align_up(d->nz, 4) : 1;
@@ -578,6 +616,10 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->off_ring = L.take((size_t)K * 2 * nslot_of(d->mode) * plane * esz);
   pl->off_acc = L.take((size_t)2 * ncomp_of(d->mode) * d->nf * plane * 16);
   pl->off_state = L.take(64);
+  if (d->probe[0] == 1) {
+    pl->probe_bytes = (size_t)4 * d->nt * d->nx * esz;
+    pl->off_probe = L.take(pl->probe_bytes);
+  }
   if (variant == kVariantSweep) {
     pl->off_tmaps = L.take(15 * 128);
     pl->L = choose_chunk(d, g_sweep_slots > 0 ? g_sweep_slots : 148 * 3);
@@ -849,11 +891,33 @@ void launch_sweep(const Params<T> &p, const SweepItem *items, int nitems, int s,
 
 // One time step of one job (s = step offset inside the K block, par = the
 // buffer holding the state at this step).
+// Line probe of the state after step s; `b` = the buffer holding it.
+template <typename T, bool EXACT> void launch_probe(oidt_ctx *ctx, Job *J, int s, int b, cudaStream_t st) {
+  const Params<T> &p = cells<T>(J)[b];
+  ProbeArgs<T> a;
+  a.ey = p.f[EY];
+  a.ez = p.f[EZ];
+  a.hy = p.f[HY];
+  a.hz = p.f[HZ];
+  a.out = reinterpret_cast<T *>(J->mem + J->pl.off_probe);
+  a.nx = J->d.nx;
+  a.nt = J->d.nt;
+  a.ie = J->d.ie;
+  a.jc = J->d.probe[1];
+  a.kc = J->d.probe[2];
+  a.sy = J->pl.nzp;
+  a.sx = (long long)J->d.ny * J->pl.nzp;
+  a.state = reinterpret_cast<const int *>(J->mem + J->pl.off_state);
+  k_probe<T, EXACT><<<(a.ie + 127) / 128, 128, 0, st>>>(a, s);
+  ctx->launches += 1;
+}
+
 template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s, int par, cudaStream_t st) {
   if (J->pl.variant == kVariantSweep) {
     launch_sweep<T, EXACT>(views<T>(J)[par], reinterpret_cast<const SweepItem *>(J->mem + J->pl.off_items),
                            J->pl.nitems, s, st);
     ctx->launches += 1;
+    if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par ^ 1, st);
     return;
   }
   Params<T> &p = cells<T>(J)[par];
@@ -867,6 +931,7 @@ template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s,
     k_2d_h<T, EXACT><<<grd, blk, 0, st>>>(p, s);
   }
   ctx->launches += 2;
+  if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par, st);
 }
 
 template <typename T, bool EXACT> void launch_fold(oidt_ctx *ctx, Job *J, int count, cudaStream_t st) {
@@ -1040,10 +1105,13 @@ template <typename T, bool EXACT> int profile_t(oidt_ctx *ctx, Job *J, int nstep
     const int par = J->parity ^ (sweep ? (s & 1) : 0);
     if (sweep) {  // one launch per step: reported as the E half, H half = 0
       cudaEventRecord(ev[q++], st);
-      launch_step<T, EXACT>(ctx, J, s, par, st);
+      launch_sweep<T, EXACT>(views<T>(J)[par], reinterpret_cast<const SweepItem *>(J->mem + J->pl.off_items),
+                             J->pl.nitems, s, st);
+      ctx->launches += 1;
       cudaEventRecord(ev[q++], st);
       cudaEventRecord(ev[q++], st);
       cudaEventRecord(ev[q++], st);
+      if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par ^ 1, st);  // untimed
       continue;
     }
     Params<T> &p = cells<T>(J)[par];
@@ -1055,6 +1123,7 @@ template <typename T, bool EXACT> int profile_t(oidt_ctx *ctx, Job *J, int nstep
       cudaEventRecord(ev[q++], st);
       k_y3_h<T, EXACT><<<grd, blk, 0, st>>>(p, s);
       cudaEventRecord(ev[q++], st);
+      if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par, st);  // untimed
     } else {
       dim3 blk(kBlock2), grd((p.ny + kBlock2 - 1) / kBlock2, p.nx);
       cudaEventRecord(ev[q++], st);
@@ -1360,6 +1429,21 @@ int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t com
   return OIDT_OK;
 }
 
+int32_t oidt_job_read_probe(oidt_ctx *ctx, uint64_t job, int32_t comp, void *out, size_t nbytes) {
+  if (!ctx || !out) return OIDT_ERR_INVALID;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  Job *J = find(ctx, job);
+  if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
+  if (!J->pl.probe_bytes) return fail(ctx, OIDT_ERR_STATE, "job has no line probe");
+  if (comp < 0 || comp > 3) return fail(ctx, OIDT_ERR_INVALID, "probe comp must be 0..3 (Ey, Ez, Hy, Hz)");
+  const size_t need = J->pl.probe_bytes / 4;
+  if (nbytes < need) return fail(ctx, OIDT_ERR_INVALID, "output needs %zu bytes", need);
+  int rc = read_common(ctx, J);
+  if (rc) return rc;
+  CU(ctx, cudaMemcpy(out, J->mem + J->pl.off_probe + comp * need, need, cudaMemcpyDeviceToHost));
+  return OIDT_OK;
+}
+
 // ---- port-window DFT readout through static device scratch -------------------
 // A variant of the staged readout that allocates nothing: the window of one
 // (port, component) accumulator is gathered into a file-scope device buffer of
@@ -1526,6 +1610,7 @@ int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_ring, 0, pl.off_acc - pl.off_ring, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_acc, 0, pl.off_state - pl.off_acc, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_state, 0, 64, st));
+  if (pl.probe_bytes) CU(ctx, cudaMemsetAsync(J->mem + pl.off_probe, 0, pl.probe_bytes, st));
   CU(ctx, cudaEventRecord(J->done, st));
   J->busy = true;
   J->steps_enqueued = 0;

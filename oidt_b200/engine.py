@@ -22,7 +22,7 @@ EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error",
            "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
            "oidt_job_query", "oidt_job_read_dft", "oidt_job_read_field", "oidt_job_write_field",
            "oidt_job_read_psi", "oidt_job_release", "oidt_job_reset", "oidt_ctx_stream", "oidt_job_profile",
-           "oidt_job_read_dft_window_static")
+           "oidt_job_read_dft_window_static", "oidt_job_read_probe")
 
 
 class OidtError(RuntimeError):
@@ -72,6 +72,7 @@ def load_library(path: str = LIB_PATH):
             "oidt_job_query": ([vp, u64, C.POINTER(i32), C.POINTER(i32)], i32),
             "oidt_job_read_dft": ([vp, u64, i32, i32, vp, C.c_size_t], i32),
             "oidt_job_read_dft_window_static": ([vp, u64, i32, i32, vp, C.c_size_t], i32),
+            "oidt_job_read_probe": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_read_field": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_write_field": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_read_psi": ([vp, u64, i32, i32, i32, vp, C.c_size_t], i32),
@@ -208,6 +209,16 @@ class Job:
         out = np.empty((self.spec.nf,) + win, dtype=np.complex128)
         self.eng._check(self.eng.lib.oidt_job_read_dft_window_static(self.eng.ctx, self.id, port, ci,
                                                                      out.ctypes.data, out.size * 2))
+        return out
+
+    PROBE_COMPS = ("ey", "ez", "hy", "hz")
+
+    def probe(self, comp) -> np.ndarray:
+        """Line-probe record [nt, nx] of one component ('ey', 'ez', 'hy',
+        'hz'), in the job's precision; rows of steps not yet run are 0."""
+        ci = self.PROBE_COMPS.index(comp) if isinstance(comp, str) else comp
+        out = np.zeros((self.spec.nt, self.spec.shape[0]), dtype=self.precision)
+        self.eng._check(self.eng.lib.oidt_job_read_probe(self.eng.ctx, self.id, ci, out.ctypes.data, out.nbytes))
         return out
 
     def field(self, name: str) -> np.ndarray:

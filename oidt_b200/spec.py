@@ -80,7 +80,7 @@ class JobDesc(C.Structure):
         ("j_src", C.c_void_p),
         ("port_pos", C.c_int32 * 2), ("win_lo", C.c_int32 * 2), ("win_hi", C.c_int32 * 2),
         ("cos_e", C.c_void_p), ("sin_e", C.c_void_p), ("cos_h", C.c_void_p), ("sin_h", C.c_void_p),
-        ("ring_steps", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("ring_steps", C.c_int32), ("reserved", C.c_int32 * 4), ("probe", C.c_int32 * 3),
     ]
 
 
@@ -143,4 +143,7 @@ def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int 
     d.ring_steps = ring_steps
     d.reserved[0] = VARIANTS[variant]
     d.reserved[1] = 0 if graphs else 1
+    probe = spec.meta.get("probe")  # (y, z) of a 3D line probe along x
+    if probe is not None:
+        d.probe[0], d.probe[1], d.probe[2] = 1, int(probe[0]), int(probe[1])
     return d, keep
