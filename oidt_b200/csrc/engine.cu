@@ -41,7 +41,7 @@ using namespace oidt;
 namespace {
 
 constexpr int kDefaultRing = 32;
-constexpr int kFoldF = 8;  // frequencies per fold thread
+constexpr int kFoldF = 7;  // frequencies per fold thread (41 = 6 x 7 - 1)
 constexpr int kBlock3Z = 32, kBlock3Y = 4;
 constexpr int kBlock2 = 128;
 constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
