@@ -206,6 +206,30 @@ def pinned_spec(spec, prec):
 # ---------------------------------------------------------------------------
 # CPU baseline (the oracle, timed on the host cores)
 # ---------------------------------------------------------------------------
+def measure_slab2d(eng):
+    """The 2D TMz slab case (400 x 200 cells, 2000 steps, float64, 21
+    frequencies): device time of a whole run after a warm-up run, CUDA events
+    on the engine stream, exact and fast arithmetic."""
+    import torch
+    from oidt_b200 import workloads as W
+    spec = W.slab2d()
+    st = torch.cuda.ExternalStream(eng.stream_handle(), device=eng.device)
+    out = {"workload": "2D TMz slab %dx%d, %d steps, nf %d" % (spec.shape + (spec.nt, spec.nf)), "dtype": "f64"}
+    for arith in ("exact", "fast"):
+        job = eng.submit(spec, arith=arith, precision=np.float64)
+        job.run().sync()
+        job.reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        job.run()
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        job.release()
+        out[arith] = {"ms_per_run": round(ms, 3), "gcell_updates_per_s": round(spec.ncells * spec.nt / ms / 1e6, 3)}
+    return out
+
+
 def cpu_baseline(spec, target_s=15.0):
     """Float64 oracle on the same workload, a bounded number of time steps."""
     from oracle import cpu as OC
@@ -314,11 +338,12 @@ def run_engine(args, ws, rank, local):
     e2e_value = whole_job_rate(ws, spec.ncells, spec.nt, e2e)
 
     # ---- batched realizations and the served mix (rank 0) ----------------
-    batched = serving = None
+    batched = serving = slab2d = None
     if rank == 0 and not args.no_extra:
         from oidt_b200 import batch as B, serve as SV
         batched = B.measure(eng, n=args.batch_n, steps=3000)
         serving = SV.measure(eng, rate_hz=20.0, duration_s=args.serve_window)
+        slab2d = measure_slab2d(eng)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -347,6 +372,7 @@ def run_engine(args, ws, rank, local):
             "gpu_launches": int(launches),
             "batched": batched,
             "serving": serving,
+            "slab2d": slab2d,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -363,7 +389,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=("engine", "reference"))
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip the batched-realization and served-mix measurements")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the batched-realization, served-mix and 2D slab measurements")
     ap.add_argument("--batch-n", type=int, default=16, help="realizations in the batched-vs-plain measurement")
     ap.add_argument("--serve-window", type=float, default=3.0, help="seconds of served-mix arrivals (20 jobs/s)")
     args = ap.parse_args()
