@@ -49,3 +49,29 @@ def test_descriptor_validation_without_device():
     d.num_cpml = 5
     d.src_lo[0] = 0  # source on the PEC rim
     assert lib.oidt_job_bytes(ctypes.byref(d), ctypes.byref(b)) == -1
+
+
+def test_line_probe_descriptor_without_device():
+    """The line probe is 3D only, needs y + 1 < ny and z + 1 < nz, and adds
+    its [4][nt][nx] record to the job's device bytes."""
+    from oidt_b200 import workloads as W
+    from oidt_b200.engine import load_library
+    from oidt_b200.spec import to_desc
+    lib = load_library()
+    spec = W.strip3d(nx=20, ny=19, nz=40, P=4, src_gap=2, port_gap=3, steps=30, nf=2, core_x_nm=120,
+                     core_y_nm=160)
+    b0, b1 = ctypes.c_uint64(), ctypes.c_uint64()
+    d, keep = to_desc(spec)
+    assert lib.oidt_job_bytes(ctypes.byref(d), ctypes.byref(b0)) == 0
+    spec.meta["probe"] = (9, 20)
+    d, keep = to_desc(spec)
+    assert list(d.probe) == [1, 9, 20] and list(d.reserved) == [0, 0, 0, 0]
+    assert lib.oidt_job_bytes(ctypes.byref(d), ctypes.byref(b1)) == 0
+    assert b1.value - b0.value >= 4 * 30 * 20 * 4  # float32 record [4][nt][nx]
+    for bad in ((1, 18, 20), (1, 9, 39), (1, -1, 20), (2, 9, 20), (0, 9, 20)):
+        d.probe[0], d.probe[1], d.probe[2] = bad
+        assert lib.oidt_job_bytes(ctypes.byref(d), ctypes.byref(b1)) == -1, bad
+    spec2 = W.slab2d(nx=60, ny=50, P=5, core_cells=6, src_x=10, ports=(15, 45), steps=10, nf=3)
+    spec2.meta["probe"] = (5, 0)
+    d2, keep2 = to_desc(spec2)
+    assert lib.oidt_job_bytes(ctypes.byref(d2), ctypes.byref(b1)) == -1  # 2D: no line probe
