@@ -287,3 +287,21 @@ def test_two_line_launcher_equals_reference_smatrix(tmp_path, batch):
     freqs, S_file, _ = read_touchstone(path)
     assert S_file.shape == S.shape
 
+
+
+def test_dft_into_caller_buffer(eng):
+    """Job.dft(out=...) reads into a caller's (here page-locked) buffer and
+    equals the allocating read; a buffer of the wrong shape is refused."""
+    import torch
+    spec = _random_cases()["yee3d_te"]()
+    job = eng.submit(spec, arith="exact", precision=np.float64)
+    job.run().sync(60000)
+    want = job.dft(1, "hy")
+    t = torch.empty(want.shape + (2,), dtype=torch.float64, pin_memory=True)
+    buf = t.numpy().view(np.complex128)[..., 0]
+    got = job.dft(1, "hy", out=buf)
+    assert got is buf
+    np.testing.assert_array_equal(buf, want)
+    with pytest.raises(ValueError):
+        job.dft(1, "hy", out=np.empty(want.shape[1:], dtype=np.complex128))
+    job.release()
