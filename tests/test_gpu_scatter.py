@@ -20,9 +20,10 @@ from oidt_b200 import scatter
 from oidt_b200.engine import Engine
 from tests import golden_io as G
 
-pytestmark = pytest.mark.gpu
-
 CASES = ["scatter_te", "scatter_tm"]
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not all(os.path.exists(os.path.join(G.GOLDEN, c + ".npz")) for c in CASES),
+                                 reason="scattering-loss fixtures not generated (tests/golden/make_golden.py)")]
 PLANE_TOL = 2e-5
 ALPHA_TOL = 1e-4
 
