@@ -30,6 +30,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/oidt.h"
@@ -63,6 +64,7 @@ template <typename T> struct ProbeArgs {
 };
 
 template <typename T, bool EXACT> __global__ void __launch_bounds__(128) k_probe(ProbeArgs<T> a, int s) {
+  pdl_wait();
   using A = Ar<T, EXACT>;
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.state[0] + s;
@@ -101,6 +103,7 @@ __device__ __forceinline__ bool block_meets_src(const Params<T> &p, int i, int j
 // plan_job rejects grids whose plane or slab sizes would not fit.
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_e(Params<T> p, int s) {
+  pdl_wait();
   const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = blockIdx.z;
   const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
   if (!block_meets_src(p, i, j0, k0)) {
@@ -186,6 +189,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_e(Params<T>
 }
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_h(Params<T> p, int s) {
+  pdl_wait();
   // planes in decreasing i: the H half starts on the E planes the E half wrote
   // last (still in L2), and ends on the planes the next E half reads first
   const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = gridDim.z - 1 - blockIdx.z;
@@ -275,6 +279,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_h(Params<T>
 
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128) k_2d_e(Params<T> p, int s) {
+  pdl_wait();
   const int j = blockIdx.x * kBlock2 + threadIdx.x, i = blockIdx.y;
   if (j >= p.ny) return;
   if (p.mode == OIDT_MODE_TM2)
@@ -284,6 +289,7 @@ __global__ void __launch_bounds__(128) k_2d_e(Params<T> p, int s) {
 }
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128) k_2d_h(Params<T> p, int s) {
+  pdl_wait();
   // rows in decreasing i (the E half's last rows are still in L2)
   const int j = blockIdx.x * kBlock2 + threadIdx.x, i = gridDim.y - 1 - blockIdx.y;
   if (j >= p.ny) return;
@@ -351,6 +357,7 @@ __device__ __forceinline__ double coloc(const FoldParams<T> &fp, int port, int c
 constexpr int kFoldChunk = 32;
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
+  pdl_wait();
   using A = Ar<double, EXACT>;
   __shared__ double2 tw[kFoldChunk][kFoldF];
   const int wj = fp.whi1 - fp.wlo1;
@@ -403,6 +410,7 @@ __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
 }
 
 __global__ void k_bump(int *state, int count) {
+  pdl_wait();
   if (threadIdx.x == 0 && blockIdx.x == 0) state[0] += count;
 }
 
@@ -882,11 +890,32 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
   return OIDT_OK;
 }
 
+// Launch of a time-step kernel with programmatic stream serialization: the
+// kernel may be scheduled while its predecessor in the stream drains, and
+// waits for it in pdl_wait() (every step kernel calls it first).  This hides
+// the gap between dependent launches, which dominates small grids.
+template <typename... KArgs, typename... Args>
+void launch_step_kernel(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                        Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, EYB, EZB, ST>(); }
 
 template <typename T, bool EXACT>
 void launch_sweep(const Params<T> &p, const SweepItem *items, int nitems, int s, cudaStream_t st) {
-  k_sweep3d<T, EXACT, EYB, EZB, ST><<<nitems, SweepGeom<T, EYB, EZB>::THREADS, sweep_smem<T>(), st>>>(p, items, s);
+  launch_step_kernel(k_sweep3d<T, EXACT, EYB, EZB, ST>, dim3(nitems), dim3(SweepGeom<T, EYB, EZB>::THREADS),
+                     sweep_smem<T>(), st, p, items, s);
 }
 
 // One time step of one job (s = step offset inside the K block, par = the
@@ -908,7 +937,7 @@ template <typename T, bool EXACT> void launch_probe(oidt_ctx *ctx, Job *J, int s
   a.sy = J->pl.nzp;
   a.sx = (long long)J->d.ny * J->pl.nzp;
   a.state = reinterpret_cast<const int *>(J->mem + J->pl.off_state);
-  k_probe<T, EXACT><<<(a.ie + 127) / 128, 128, 0, st>>>(a, s);
+  launch_step_kernel(k_probe<T, EXACT>, dim3((a.ie + 127) / 128), dim3(128), 0, st, a, s);
   ctx->launches += 1;
 }
 
@@ -923,12 +952,12 @@ template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s,
   Params<T> &p = cells<T>(J)[par];
   if (J->d.mode == OIDT_MODE_YEE3D) {
     dim3 blk(kBlock3Z, kBlock3Y), grd((p.nz + kBlock3Z - 1) / kBlock3Z, (p.ny + kBlock3Y - 1) / kBlock3Y, p.nx);
-    k_y3_e<T, EXACT><<<grd, blk, 0, st>>>(p, s);
-    k_y3_h<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+    launch_step_kernel(k_y3_e<T, EXACT>, grd, blk, 0, st, p, s);
+    launch_step_kernel(k_y3_h<T, EXACT>, grd, blk, 0, st, p, s);
   } else {
     dim3 blk(kBlock2), grd((p.ny + kBlock2 - 1) / kBlock2, p.nx);
-    k_2d_e<T, EXACT><<<grd, blk, 0, st>>>(p, s);
-    k_2d_h<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+    launch_step_kernel(k_2d_e<T, EXACT>, grd, blk, 0, st, p, s);
+    launch_step_kernel(k_2d_h<T, EXACT>, grd, blk, 0, st, p, s);
   }
   ctx->launches += 2;
   if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par, st);
@@ -939,8 +968,8 @@ template <typename T, bool EXACT> void launch_fold(oidt_ctx *ctx, Job *J, int co
   const int wj = fp.whi1 - fp.wlo1;
   const int wi = J->d.mode == OIDT_MODE_YEE3D ? fp.whi0 - fp.wlo0 : 1;
   dim3 grd((wi * wj + 127) / 128, (fp.nf + kFoldF - 1) / kFoldF, 2 * fp.ncomp);
-  k_fold<T, EXACT><<<grd, 128, 0, st>>>(fp, count);
-  k_bump<<<1, 32, 0, st>>>(reinterpret_cast<int *>(J->mem + J->pl.off_state), count);
+  launch_step_kernel(k_fold<T, EXACT>, grd, dim3(128), 0, st, fp, count);
+  launch_step_kernel(k_bump, dim3(1), dim3(32), 0, st, reinterpret_cast<int *>(J->mem + J->pl.off_state), count);
   ctx->launches += 2;
 }
 

@@ -53,6 +53,15 @@ template <> struct Ar<double, false> {
 };
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch.  The kernels of a time step are launched with
+// the programmatic-serialization attribute, so a kernel may start while the
+// previous kernel in its stream drains; each calls pdl_wait() before its first
+// global-memory access, which returns once that kernel has completed and its
+// writes are visible.  Launched without the attribute, it returns at once.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
 // Job parameters (device-resident copy for batched launches).
 // ---------------------------------------------------------------------------
 template <typename T> struct Params {

@@ -132,6 +132,7 @@ __device__ __forceinline__ int ss(int code) { return code >> 24; }
 template <typename T, bool EXACT, int TBY, int TBZ, int S>
 __global__ void __launch_bounds__(TBY *TBZ, sizeof(T) == 4 ? 4 : 2)
     k_sweep3d(const __grid_constant__ Params<T> p, const SweepItem *__restrict__ items, int s) {
+  pdl_wait();
   static_assert(S >= 3, "the stage refilled after plane u must differ from those of planes u+1, u+2");
   using G = SweepGeom<T, TBY, TBZ>;
   using A = Ar<T, EXACT>;
