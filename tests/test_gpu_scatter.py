@@ -104,9 +104,16 @@ def _oracle64(over, prof):
     return s
 
 
-def test_batched_realizations_equal_plain_runs(eng):
+def _rough_cfg():
+    """The fixture's tiny grid with roughness of about two cells (the
+    default 15 nm is a fifth of a 73 nm cell: most draws leave the staircase
+    mask unchanged)."""
     _, over, _ = _load("scatter_te")
-    cfg = scatter.config(**over)
+    return scatter.config(**dict(over, rough_std=150e-9, rough_acl=300e-9))
+
+
+def test_batched_realizations_equal_plain_runs(eng):
+    cfg = _rough_cfg()
     profs = scatter.realization_profiles(cfg, 3, master_seed=4)
     _, plain = scatter.run(eng, cfg, profs, batched=False)
     _, batch = scatter.run(eng, cfg, profs, batched=True)
@@ -120,8 +127,7 @@ def test_batched_realizations_equal_plain_runs(eng):
 def test_batched_realizations_split_by_budget():
     """With a context budget that holds two of three jobs, the batched path
     runs them in two groups and still equals the one-at-a-time runs."""
-    _, over, _ = _load("scatter_te")
-    cfg = scatter.config(**over)
+    cfg = _rough_cfg()
     profs = scatter.realization_profiles(cfg, 3, master_seed=6)
     probe = Engine(0)
     need = probe.job_bytes(scatter.build_spec(cfg, profs[0]), precision=np.float32)
