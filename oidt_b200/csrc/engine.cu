@@ -670,7 +670,12 @@ struct BatchPlan {  // cached multi-job composition: one CUDA graph per K-step b
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
   int K = 0;
+  unsigned long long last_use = 0;
 };
+// Compositions kept: a serving loop that advances its jobs in a few groups
+// (small jobs take more steps per tick than large ones) replays each group's
+// graph without re-capturing it while the group's membership is unchanged.
+constexpr int kBatchCache = 8;
 
 constexpr int kAuxStreams = 16;
 
@@ -688,7 +693,8 @@ struct oidt_ctx {
   std::mutex mu;
   std::string err;
   long long launches = 0;
-  BatchPlan batch;
+  BatchPlan batch[kBatchCache];
+  unsigned long long batch_clock = 0;
 };
 
 namespace {
@@ -1052,7 +1058,6 @@ template <typename T, bool EXACT> int batch_block(oidt_ctx *ctx, std::vector<Job
 template <typename T, bool EXACT>
 int batch_t(oidt_ctx *ctx, std::vector<Job *> &js, int nsteps) {
   cudaStream_t st = ctx->stream;
-  BatchPlan &bp = ctx->batch;
   const int K = js[0]->pl.K;
   for (Job *j : js) {
     if (j->pl.K != K) return fail(ctx, OIDT_ERR_INVALID, "batched jobs must share ring_steps");
@@ -1063,12 +1068,22 @@ int batch_t(oidt_ctx *ctx, std::vector<Job *> &js, int nsteps) {
     std::vector<uint64_t> ids;
     std::vector<int> pars;
     for (Job *j : js) ids.push_back(j->id), pars.push_back(j->parity);
-    if (bp.ids != ids || bp.pars != pars || bp.K != K) {
-      drop_batch(bp);
-      bp.ids = ids;
-      bp.pars = pars;
-      bp.K = K;
+    // the cached composition of these jobs at these parities, else the least
+    // recently used slot
+    BatchPlan *hit = nullptr, *lru = &ctx->batch[0];
+    for (BatchPlan &c : ctx->batch) {
+      if (c.K == K && c.ids == ids && c.pars == pars) hit = &c;
+      if (c.last_use < lru->last_use) lru = &c;
     }
+    if (!hit) {
+      drop_batch(*lru);
+      lru->ids = ids;
+      lru->pars = pars;
+      lru->K = K;
+      hit = lru;
+    }
+    BatchPlan &bp = *hit;
+    bp.last_use = ++ctx->batch_clock;
     const int cnt = std::min(K, left);
     int rc = OIDT_OK;
     if (cnt == K && (K & 1) == 0) {
@@ -1284,7 +1299,7 @@ int32_t oidt_destroy(oidt_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (auto &kv : ctx->jobs) destroy_job(ctx, kv.second);
     ctx->jobs.clear();
-    drop_batch(ctx->batch);
+    for (BatchPlan &bp : ctx->batch) drop_batch(bp);
     cudaStreamSynchronize(ctx->stream);
     for (int a = 0; a < kAuxStreams; ++a) {
       cudaStreamSynchronize(ctx->aux[a]);
@@ -1613,7 +1628,8 @@ int32_t oidt_job_release(oidt_ctx *ctx, uint64_t job) {
   if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
   CU(ctx, cudaSetDevice(ctx->device));
   CU(ctx, cudaEventSynchronize(J->done));
-  if (std::find(ctx->batch.ids.begin(), ctx->batch.ids.end(), job) != ctx->batch.ids.end()) drop_batch(ctx->batch);
+  for (BatchPlan &bp : ctx->batch)
+    if (std::find(bp.ids.begin(), bp.ids.end(), job) != bp.ids.end()) drop_batch(bp);
   ctx->in_use -= J->pl.total;
   ctx->jobs.erase(job);
   destroy_job(ctx, J);

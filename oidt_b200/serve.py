@@ -6,9 +6,13 @@ Requests (a SimSpec each, or a builder for one) arrive over time.  The loop
    allows (``oidt_job_create`` refuses with OIDT_ERR_BUDGET otherwise; the
    request then waits for memory to be freed) -- admission copies the job's
    coefficients to the device while earlier jobs keep running;
-2. advances every admitted job together by one tick of ``tick`` steps in
-   multi-job launches (``oidt_batch_advance``); jobs with fewer steps left
-   finish on their own in the same stream;
+2. advances every admitted job in one tick of multi-job launches
+   (``oidt_batch_advance``), each by its share of the tick: ``tick`` steps
+   times the power of two nearest below (largest active job's cells / its
+   cells), at most 64x.  Every job then gets about the same cell-updates per
+   tick, so a small job (a 2D run beside 3D ones) leaves after a tick or two
+   instead of queuing behind the large jobs' steps; total work and every
+   result are unchanged (``fair_share=False`` gives every job ``tick`` steps);
 3. retires finished jobs: reads their port DFTs, computes S11/S21, records
    latency = finish time - arrival time, frees their memory.
 
@@ -54,14 +58,18 @@ class Result:
 
 class Server:
     def __init__(self, engine: Engine, tick: int = 64, precision=np.float32, arith: str = "fast",
-                 keep_dfts: bool = False, ring_steps: int = 32):
+                 keep_dfts: bool = False, ring_steps: int = 32, fair_share: bool = True, max_boost_log2: int = 6):
+        if tick % ring_steps:
+            raise ValueError("tick must be a multiple of ring_steps")
         self.eng = engine
         self.tick = tick
+        self.fair_share = fair_share
+        self.max_boost_log2 = max_boost_log2
         self.precision = precision
         self.arith = arith
         self.keep_dfts = keep_dfts
         self.ring = ring_steps
-        self.active = []   # (request, job[, incident job])
+        self.active = []   # (request, job, incident job or None, admit time)
         self.results = []
         self.refused = 0
 
@@ -97,22 +105,40 @@ class Server:
         for x in jobs:
             x.release()
 
+    def quota(self, cells: int, ref_cells: int) -> int:
+        """Steps per tick of a job of ``cells`` cells beside a largest active
+        job of ``ref_cells``: ``tick`` times 2^floor(log2(ref / cells)), at
+        most 2^max_boost_log2."""
+        if not self.fair_share:
+            return self.tick
+        r = max(1, int(ref_cells // max(1, cells)))
+        return self.tick << min(self.max_boost_log2, r.bit_length() - 1)
+
     def _tick(self):
         """Enqueue one tick for every admitted request with steps left; returns
-        the requests whose last steps are now enqueued."""
+        the requests whose last steps are now enqueued.  Whole ring blocks go
+        through multi-job launches: block b advances every job with more than
+        b blocks in its share, so the groups shrink as the small shares end
+        (each group's graph is cached by the engine); a share's last partial
+        block, if any, runs alone."""
         jobs = []
         for (req, j, ji, adm) in self.active:
             jobs += [x for x in (j, ji) if x is not None and x.steps < x.spec.nt]
-        left = [x.spec.nt - x.steps for x in jobs]
-        full = [x for x, l in zip(jobs, left) if l >= self.tick]
-        rest = [(x, l) for x, l in zip(jobs, left) if 0 < l < self.tick]
-        by_prec = {}
-        for x in full:
-            by_prec.setdefault(str(x.precision), []).append(x)
-        for group in by_prec.values():
-            self.eng.batch_advance(group, self.tick)
-        for x, l in rest:
-            x.advance(l)
+        if jobs:
+            ref = max(x.spec.ncells for x in jobs)
+            share = [min(x.spec.nt - x.steps, self.quota(x.spec.ncells, ref)) for x in jobs]
+            K = self.ring
+            blocks = [n // K for n in share]
+            for b in range(max(blocks)):
+                by_prec = {}
+                for x, nb in zip(jobs, blocks):
+                    if nb > b:
+                        by_prec.setdefault(str(x.precision), []).append(x)
+                for group in by_prec.values():
+                    self.eng.batch_advance(group, K)
+            for x, n in zip(jobs, share):
+                if n % K:
+                    x.advance(n % K)
         done, keep = [], []
         for e in self.active:
             (done if all(x.steps >= x.spec.nt for x in e[1:3] if x is not None) else keep).append(e)
@@ -184,9 +210,15 @@ def requests_from_mix(mix, nf=21, precision=np.float32):
     return out
 
 
-def measure(eng: Engine, rate_hz=20.0, duration_s=3.0, seed=0, tick=64, max_wall=300.0):
+def measure(eng: Engine, rate_hz=20.0, duration_s=3.0, seed=0, tick=64, max_wall=300.0, warmup=True):
     """Serve the first ``duration_s`` seconds of the served mix at ``rate_hz``
-    with arrivals honoured on the wall clock; latency and throughput."""
+    with arrivals honoured on the wall clock; latency and throughput.  A
+    server pays its start-up once (kernel module loads, the first graph
+    instantiations, device memory pool growth); with ``warmup`` the same
+    length of the mix with another seed is served first, untimed."""
+    if warmup:
+        Server(eng, tick=tick).run(requests_from_mix(W.serving_mix(rate_hz=rate_hz, duration_s=duration_s,
+                                                                   seed=seed + 1)), realtime=True, max_wall=max_wall)
     reqs = requests_from_mix(W.serving_mix(rate_hz=rate_hz, duration_s=duration_s, seed=seed))
     srv = Server(eng, tick=tick)
     t0 = time.perf_counter()
@@ -198,5 +230,7 @@ def measure(eng: Engine, rate_hz=20.0, duration_s=3.0, seed=0, tick=64, max_wall
     return {"rate_hz": rate_hz, "arrival_window_s": duration_s, "requests": len(reqs), "completed": len(res),
             "p50_s": round(st["p50_s"], 3), "p99_s": round(st["p99_s"], 3), "mean_s": round(st["mean_s"], 3),
             "wall_s": round(wall, 3), "jobs_per_s": round(len(res) / wall, 3),
-            "gcell_updates_per_s": round(cells / wall / 1e9, 3), "admission_refusals": srv.refused}
+            "gcell_updates_per_s": round(cells / wall / 1e9, 3), "admission_refusals": srv.refused,
+            "policy": "work-fair shares, cap 64x" if srv.fair_share else "equal steps per tick",
+            "warmed_up": bool(warmup)}
 

@@ -86,3 +86,51 @@ def test_late_arrivals_join_running_batch():
     srv.run(reqs[:1] + [Request(2, 0.0, FakeSpec(nt=128, bytes_=1))], realtime=False)
     sizes = [e[1] for e in eng.log if e[0] == "batch"]
     assert sizes[0] == 2 and 1 in sizes  # both ran together, then the long one alone
+
+
+def test_fair_share_lets_small_jobs_leave_first():
+    """Each job's steps per tick scale with (largest cells / its cells) in
+    powers of two, capped at 64x: beside a large job, small jobs finish in
+    the first tick while the large one needs many; every job still advances
+    exactly its step count, in whole ring blocks plus one partial block."""
+    class TickEngine(FakeEngine):
+        ticks = 0
+
+        def mark(self):
+            TickEngine.ticks += 1
+            return super().mark()
+
+    def finish_ticks(fair):
+        TickEngine.ticks = 0
+        eng = TickEngine(budget=10 ** 9)
+        reqs = [Request(0, 0.0, FakeSpec(nt=2000, bytes_=1, shape=(400, 400)))]
+        reqs += [Request(k, 0.0, FakeSpec(nt=1990 + k, bytes_=1)) for k in range(1, 5)]
+        srv = Server(eng, tick=64, fair_share=fair)
+        order = []
+        orig = srv._finish
+
+        def record(entry, t0):
+            order.append((entry[0].rid, TickEngine.ticks))
+            orig(entry, t0)
+        srv._finish = record
+        srv.run(reqs, realtime=False, depth=1)
+        assert all(j.steps == j.spec.nt for j in eng.jobs)
+        return dict(order)
+
+    fair, plain = finish_ticks(True), finish_ticks(False)
+    assert all(fair[k] == 1 for k in range(1, 5)) and fair[0] >= 30
+    assert all(plain[k] >= 30 for k in range(1, 5))
+    srv = Server(FakeEngine(1), tick=64)
+    assert srv.quota(160000, 160000) == 64 and srv.quota(1200, 160000) == 64 * 64
+    assert srv.quota(40000, 160000) == 64 * 4 and srv.quota(30000, 160000) == 64 * 4
+
+
+def test_fair_share_groups_share_launches():
+    """Jobs of one size class advance together: with equal sizes every block
+    is one multi-job launch of all of them."""
+    eng = FakeEngine(budget=10 ** 9)
+    reqs = [Request(k, 0.0, FakeSpec(nt=320, bytes_=1)) for k in range(3)]
+    Server(eng, tick=64).run(reqs, realtime=False)
+    batches = [e for e in eng.log if e[0] == "batch"]
+    assert batches and all(n_jobs == 3 and n == 32 for _, n_jobs, n in batches)
+    assert sum(n for _, _, n in batches) == 320
