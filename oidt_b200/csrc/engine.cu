@@ -7,15 +7,18 @@
 // reciprocals, CPML psi slabs in the reference's PSI_<F>_<A><LO|HI> shapes,
 // the source waveform, float64 twiddle tables [nf][nt], the capture ring
 // [K][port][slot][plane], float64 complex DFT accumulators
-// [port][comp][nf][plane], and for 3D a second field buffer and a second
-// E-psi buffer (the plane sweep writes the other buffer each step).
+// [port][comp][nf][plane], an optional line-probe record [4][nt][nx], and for
+// the 3D plane-sweep form a second field buffer and a second E-psi buffer (it
+// writes the other buffer each step).
 //
-// A 3D time step is one launch of the plane sweep (sweep3d.cuh) over the job's
-// work items; 2D steps (and the 3D per-cell variant) are two launches (E
-// half, H half; kernels.cuh).  Every K steps a fold kernel turns the captured
-// port planes into float64 DFT updates and a one-thread kernel advances the
-// step counter, so a K-step block is a fixed launch sequence that is captured
-// once into a CUDA graph and replayed.
+// A time step is two per-cell launches (E half, H half; kernels.cuh) -- or,
+// for 3D jobs that ask for it, one plane-sweep launch over the job's work
+// items (sweep3d.cuh) -- then the line probe if the job has one.  Every K
+// steps a fold kernel turns the captured port planes into float64 DFT updates
+// and a one-thread kernel advances the step counter, so a K-step block is a
+// fixed launch sequence, captured once into a CUDA graph and replayed.  The
+// step kernels are launched with programmatic stream serialization and wait
+// for their predecessor in pdl_wait().
 #include <cuda.h>
 #include <cuda_runtime.h>
 
