@@ -680,7 +680,7 @@ struct BatchPlan {  // cached multi-job composition: one CUDA graph per K-step b
 // graph without re-capturing it while the group's membership is unchanged.
 constexpr int kBatchCache = 8;
 
-constexpr int kAuxStreams = 16;
+constexpr int kAuxStreams = 64;  // a served request is two jobs; the mix keeps ~40 active
 
 }  // namespace
 
