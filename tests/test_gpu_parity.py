@@ -40,16 +40,18 @@ def _fixture_cases():
     return out
 
 
-@pytest.mark.parametrize("variant", ["sweep", "cell"])
-@pytest.mark.parametrize("case", _fixture_cases())
+def _case_variants():
+    """3D runs under both launch forms (plane sweep, per-cell); 2D has one."""
+    return [(c, v) for c in _fixture_cases() for v in (("sweep", "cell") if c.startswith("yee3d") else ("cell",))]
+
+
+@pytest.mark.parametrize("case,variant", _case_variants())
 def test_exact_f64_equals_reference_device_arrays(eng, case, variant):
     """Engine float64 EXACT == the reference's recorded device arrays."""
     from oidt_b200.refsetup import build_spec
     z = G.load(case)
     usr = G.usr_of(z)
     mode = case.split("_")[0]
-    if mode != "yee3d" and variant == "sweep":
-        pytest.skip("2D solvers have one launch form")
     for (line, d, kind) in G.sims_of(z):
         tag = "%d%s%s" % (line, d, kind)
         spec = build_spec(usr, mode, line, d, kind, profiles=G.profiles_of(z))
