@@ -101,7 +101,12 @@ typedef struct oidt_job_desc {
   /* reserved[0]: 3D launch form, 0 = per-cell E-half / H-half launches,
    *              1 = plane sweep (one launch per step);
    * reserved[1]: 1 = launch every step directly (no CUDA-graph replay);
-   * others must be 0. */
+   * reserved[2]: 3D per-cell form only: rows of a block's 32 x rows tile,
+   *              2, 4 or 8 (0 = 4);
+   * reserved[3]: 3D plane sweep only: march depth, the x-planes of one work
+   *              item (0 = the engine's makespan estimate).
+   * None of these changes results; they are launch choices, measured per
+   * grid shape by the host's tuner.  Other values are OIDT_ERR_INVALID. */
   int32_t reserved[4];
   /* 3D time-domain line probe, the wave-impedance runs' recording
    * (FDTD/GPU/FDTD_3D/wave_impedance/fdtd_main.py:298-299, fdtd_funcs.py:

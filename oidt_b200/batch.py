@@ -13,6 +13,9 @@ source, not on the roughness or the guide length, so:
 * :func:`run_batched` -- every rough run plus one shared incident run per
   cross-section advance together in multi-job launches (one branch per job,
   K-step blocks replayed from a CUDA graph).
+
+Both take an optional :class:`oidt_b200.tune.Tuner`; each job is then launched
+with the choices measured for its shape (results are unchanged by them).
 """
 from __future__ import annotations
 
@@ -52,14 +55,27 @@ def _dfts(job):
     return {(p, c): job.dft(p, c) for p in (0, 1) for c in range(4)}
 
 
-def run_batched(eng: Engine, rset, precision=np.float32, ring_steps=32):
+def _choice(tuner, spec, precision, ring_steps):
+    return tuner.choose(spec, precision, ring_steps=ring_steps) if tuner is not None else {}
+
+
+def tune_set(tuner, rset, precision=np.float32, ring_steps=32):
+    """Measure the launch choices of every shape in the set (untimed work
+    before a timed run)."""
+    roughs, keys, incidents = rset
+    for s in list(roughs) + list(incidents.values()):
+        tuner.choose(s, precision, ring_steps=ring_steps)
+
+
+def run_batched(eng: Engine, rset, precision=np.float32, ring_steps=32, tuner=None):
     """Advance every rough run and the shared incident runs together.
     Returns (seconds, [S dict per realization])."""
     roughs, keys, incidents = rset
     t0 = time.perf_counter()
     inc_keys = list(incidents)
     specs = roughs + [incidents[k] for k in inc_keys]
-    jobs = [eng.submit(s, precision=precision, ring_steps=ring_steps) for s in specs]
+    jobs = [eng.submit(s, precision=precision, ring_steps=ring_steps, **_choice(tuner, s, precision, ring_steps))
+            for s in specs]
     steps = min(s.nt for s in specs)
     eng.batch_advance(jobs, steps)
     for j in jobs:
@@ -74,16 +90,17 @@ def run_batched(eng: Engine, rset, precision=np.float32, ring_steps=32):
     return time.perf_counter() - t0, res
 
 
-def run_plain(eng: Engine, rset, precision=np.float32):
+def run_plain(eng: Engine, rset, precision=np.float32, tuner=None):
     """One run at a time, launched step by step: each realization's rough
     run, then its own incident run."""
     roughs, keys, incidents = rset
     t0 = time.perf_counter()
     res = []
     for spec_r, key in zip(roughs, keys):
-        jr = eng.submit(spec_r, precision=precision, graphs=False)
+        jr = eng.submit(spec_r, precision=precision, graphs=False, **_choice(tuner, spec_r, precision, 32))
         jr.run().sync()
-        ji = eng.submit(incidents[key], precision=precision, graphs=False)
+        ji = eng.submit(incidents[key], precision=precision, graphs=False,
+                        **_choice(tuner, incidents[key], precision, 32))
         ji.run().sync()
         res.append(forward_s(spec_r, _dfts(ji), _dfts(jr)))
         jr.release()
@@ -96,17 +113,27 @@ def s21_loss_db(results):
     return np.array([float(np.mean(-20 * np.log10(np.abs(r["S21"])))) for r in results])
 
 
-def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0):
+def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0, tuned=True):
     """Realizations/s of the batched path against the plain one-run-at-a-time
     path on ``n`` realizations drawn like the batched stochastic set (uneven
     grids), and the largest |S21 difference| between the two (the same
-    arithmetic on the same runs, so 0 is expected)."""
+    arithmetic on the same runs, so 0 is expected).  With ``tuned``, every
+    shape's launch choice is measured first (untimed) and both paths use it,
+    so the ratio is that of batching alone."""
     rset = realization_set(W.batch_configs(n=n, master_seed=master_seed, steps=steps), nf=nf)
     roughs, keys, incidents = rset
     plain_cells = sum(r.ncells * r.nt + incidents[k].ncells * incidents[k].nt for r, k in zip(roughs, keys))
     batched_cells = sum(r.ncells * r.nt for r in roughs) + sum(s.ncells * s.nt for s in incidents.values())
-    t_plain, s_plain = run_plain(eng, rset)
-    t_batch, s_batch = run_batched(eng, rset)
+    tuner = None
+    t_tune = 0.0
+    if tuned:
+        from .tune import Tuner
+        tuner = Tuner(eng)
+        t0 = time.perf_counter()
+        tune_set(tuner, rset)
+        t_tune = time.perf_counter() - t0
+    t_plain, s_plain = run_plain(eng, rset, tuner=tuner)
+    t_batch, s_batch = run_batched(eng, rset, tuner=tuner)
     d = max(float(np.max(np.abs(a["S21"] - b["S21"]))) for a, b in zip(s_plain, s_batch))
     loss = s21_loss_db(s_batch)
     return {"realizations": n, "steps": steps, "nf": nf, "shared_incident_runs": len(incidents),
@@ -114,4 +141,17 @@ def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0):
             "plain_s": round(t_plain, 3), "batched_s": round(t_batch, 3),
             "plain_realizations_per_s": round(n / t_plain, 3), "batched_realizations_per_s": round(n / t_batch, 3),
             "speedup": round(t_plain / t_batch, 3), "max_abs_dS21_batched_vs_plain": d,
-            "s21_loss_db_mean": float(np.mean(loss)), "s21_loss_db_std": float(np.std(loss))}
+            "s21_loss_db_mean": float(np.mean(loss)), "s21_loss_db_std": float(np.std(loss)),
+            "launch_tuning": None if tuner is None else {
+                "seconds": round(t_tune, 3), "shapes": len(tuner.table),
+                "choices": _histogram(tuner, rset)}}
+
+
+def _histogram(tuner, rset, precision=np.float32):
+    from .tune import label
+    roughs, keys, incidents = rset
+    h = {}
+    for s in list(roughs) + list(incidents.values()):
+        c = label(tuner.choose(s, precision))
+        h[c] = h.get(c, 0) + 1
+    return h

@@ -46,7 +46,7 @@ namespace {
 
 constexpr int kDefaultRing = 32;
 constexpr int kFoldF = 7;  // frequencies per fold thread (41 = 6 x 7 - 1)
-constexpr int kBlock3Z = 32, kBlock3Y = 4;
+constexpr int kBlock3Z = 32, kRowsDefault = 4;  // 3D per-cell tile: 32 (k) x rows (j), rows 2, 4 or 8
 constexpr int kBlock2 = 128;
 constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
 constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread box
@@ -86,30 +86,30 @@ template <typename T, bool EXACT> __global__ void __launch_bounds__(128) k_probe
 // ---------------------------------------------------------------------------
 // Per-cell launches (2D, and the 3D per-cell variant): in place.
 // ---------------------------------------------------------------------------
-// A block of the 3D per-cell launches covers kBlock3Z (k) x kBlock3Y (j) cells
-// of one x-plane; each warp is one (i, j) row of 32 consecutive k.  Blocks
+// A block of the 3D per-cell launches covers kBlock3Z (k) x BY (j) cells of
+// one x-plane (BY = the job's tile rows: 2, 4 or 8); each warp is one (i, j) row of 32 consecutive k.  Blocks
 // away from the source box run the range-masked body: the three curl
 // updates, then the CPML terms -- x and y slabs uniform over the warp, z slab
 // per lane -- with each component stored where its (i, j, k) range holds
 // (operation order as y3_e_compute / y3_h_compute, which they equal cell by
 // cell).  Blocks meeting the source box run the general per-cell code.
-template <typename T>
+template <int BY, typename T>
 __device__ __forceinline__ bool block_meets_src(const Params<T> &p, int i, int j0, int k0) {
   // the source box widened by one cell below in i and k (the E CPML of Ex and
   // Ez reads the Hy source at k + 1 and i + 1)
-  return p.src_field >= 0 && i >= p.slo[0] - 1 && i < p.shi[0] && j0 < p.shi[1] && j0 + kBlock3Y > p.slo[1] &&
+  return p.src_field >= 0 && i >= p.slo[0] - 1 && i < p.shi[0] && j0 < p.shi[1] && j0 + BY > p.slo[1] &&
          k0 < p.shi[2] && k0 + kBlock3Z > p.slo[2] - 1;
 }
 
 // Interior warps address every grid array as (per-plane base, uniform over
 // the block) + (32-bit offset inside the plane), and the CPML slabs likewise;
 // plan_job rejects grids whose plane or slab sizes would not fit.
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_e(Params<T> p, int s) {
+template <typename T, bool EXACT, int BY>
+__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 4 ? 64 : 32) / BY) k_y3_e(Params<T> p, int s) {
   pdl_wait();
-  const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = blockIdx.z;
+  const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * BY, i = blockIdx.z;
   const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
-  if (!block_meets_src(p, i, j0, k0)) {
+  if (!block_meets_src<BY>(p, i, j0, k0)) {
     // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
     // read below stays inside the grid arrays
     if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
@@ -190,14 +190,14 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_e(Params<T>
   if (k >= p.nz || j >= p.ny) return;
   y3_e_cell<T, EXACT>(p, i, j, k, p.state[0] + s, s);
 }
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 16 : 8) k_y3_h(Params<T> p, int s) {
+template <typename T, bool EXACT, int BY>
+__global__ void __launch_bounds__(32 * BY, (sizeof(T) == 4 ? 64 : 32) / BY) k_y3_h(Params<T> p, int s) {
   pdl_wait();
   // planes in decreasing i: the H half starts on the E planes the E half wrote
   // last (still in L2), and ends on the planes the next E half reads first
-  const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * kBlock3Y, i = gridDim.z - 1 - blockIdx.z;
+  const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * BY, i = gridDim.z - 1 - blockIdx.z;
   const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
-  if (!block_meets_src(p, i, j0, k0)) {
+  if (!block_meets_src<BY>(p, i, j0, k0)) {
     // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
     // read below stays inside the grid arrays (ib, jb >= 1)
     if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
@@ -469,6 +469,7 @@ struct JobPlan {
   size_t off_probe, probe_bytes;  // line probe [4][nt][nx] (probe_bytes = 0: none)
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
+  int rows;  // 3D per-cell tile rows
 };
 
 // Flags of the work item whose E box starts at (y0 - 1, z0 - 1) (rows
@@ -520,12 +521,9 @@ std::vector<SweepItem> sweep_items(const oidt_job_desc *d, int L) {
 // March depth: the chunk length L minimising the estimated makespan of one
 // step, (total plane iterations) / (resident CTAs) + (one item's length);
 // an item of L planes iterates L + 1 times (the E halo plane x0 - 1).
-// OIDT_SWEEP_L overrides.  `slots` = SMs x resident CTAs per SM.
+// `slots` = SMs x resident CTAs per SM.  A descriptor's reserved[3] > 0
+// replaces this estimate (the tuner's measured choice).
 int choose_chunk(const oidt_job_desc *d, int slots) {
-  if (const char *e = getenv("OIDT_SWEEP_L")) {
-    int v = atoi(e);
-    if (v > 0) return v;
-  }
   const int planes = d->ie - d->ib;
   const long long tiles = (long long)((d->ny + TY - 1) / TY) * ((d->nz + TZ - 1) / TZ);
   double best = 1e300;
@@ -594,7 +592,15 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   } else if (d->probe[1] != 0 || d->probe[2] != 0) {
     return bad("probe[1..2] must be 0 without a probe");
   }
+  if (d->reserved[0] != kVariantCell && d->reserved[0] != kVariantSweep) return bad("reserved[0]: launch form 0 or 1");
+  if (d->reserved[1] != 0 && d->reserved[1] != 1) return bad("reserved[1]: 0 or 1");
   const int variant = is3 && d->reserved[0] == kVariantSweep ? kVariantSweep : kVariantCell;
+  const int rows = d->reserved[2] == 0 ? kRowsDefault : d->reserved[2];
+  if (rows != 2 && rows != 4 && rows != 8) return bad("reserved[2]: tile rows 0 (default), 2, 4 or 8");
+  if (d->reserved[2] != 0 && !(is3 && variant == kVariantCell))
+    return bad("reserved[2] (tile rows) applies to the 3D per-cell form");
+  if (d->reserved[3] < 0 || (d->reserved[3] != 0 && !(is3 && variant == kVariantSweep)))
+    return bad("reserved[3] (march depth) is >= 0 and applies to the 3D plane sweep");
   const int esz = d->precision == OIDT_F32 ? 4 : 8;
   const int nzp = is3 ? (int)align_up(d->nz, 4) : 1;
   const long long N = (long long)d->nx * d->ny * nzp;
@@ -633,7 +639,8 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   }
   if (variant == kVariantSweep) {
     pl->off_tmaps = L.take(15 * 128);
-    pl->L = choose_chunk(d, g_sweep_slots > 0 ? g_sweep_slots : 148 * 3);
+    pl->L = d->reserved[3] > 0 ? std::min(d->reserved[3], d->ie - d->ib)
+                               : choose_chunk(d, g_sweep_slots > 0 ? g_sweep_slots : 148 * 3);
     pl->nitems = (int)sweep_items(d, pl->L).size();
     pl->off_items = L.take((size_t)pl->nitems * sizeof(SweepItem));
   }
@@ -641,6 +648,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->N = N;
   pl->plane = plane;
   pl->K = K;
+  pl->rows = rows;
   pl->esz = esz;
   pl->nzp = nzp;
   pl->nbuf = nbuf;
@@ -919,6 +927,23 @@ void launch_step_kernel(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sm
   cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
+// One 3D per-cell half-step (H = false: E, true: H) with blocks of 32 x BY
+// cells; pdl = false launches without the programmatic-serialization
+// attribute (the per-launch timing path).
+template <typename T, bool EXACT, int BY>
+void y3_half_by(bool H, bool pdl, const Params<T> &p, int s, cudaStream_t st) {
+  const dim3 blk(kBlock3Z, BY), grd((p.nz + kBlock3Z - 1) / kBlock3Z, (p.ny + BY - 1) / BY, p.nx);
+  void (*kern)(Params<T>, int) = H ? k_y3_h<T, EXACT, BY> : k_y3_e<T, EXACT, BY>;
+  if (pdl) launch_step_kernel(kern, grd, blk, 0, st, p, s);
+  else kern<<<grd, blk, 0, st>>>(p, s);
+}
+template <typename T, bool EXACT>
+void y3_half(int rows, bool H, bool pdl, const Params<T> &p, int s, cudaStream_t st) {
+  if (rows == 2) y3_half_by<T, EXACT, 2>(H, pdl, p, s, st);
+  else if (rows == 8) y3_half_by<T, EXACT, 8>(H, pdl, p, s, st);
+  else y3_half_by<T, EXACT, 4>(H, pdl, p, s, st);
+}
+
 template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, EYB, EZB, ST>(); }
 
 template <typename T, bool EXACT>
@@ -960,9 +985,8 @@ template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s,
   }
   Params<T> &p = cells<T>(J)[par];
   if (J->d.mode == OIDT_MODE_YEE3D) {
-    dim3 blk(kBlock3Z, kBlock3Y), grd((p.nz + kBlock3Z - 1) / kBlock3Z, (p.ny + kBlock3Y - 1) / kBlock3Y, p.nx);
-    launch_step_kernel(k_y3_e<T, EXACT>, grd, blk, 0, st, p, s);
-    launch_step_kernel(k_y3_h<T, EXACT>, grd, blk, 0, st, p, s);
+    y3_half<T, EXACT>(J->pl.rows, false, true, p, s, st);
+    y3_half<T, EXACT>(J->pl.rows, true, true, p, s, st);
   } else {
     dim3 blk(kBlock2), grd((p.ny + kBlock2 - 1) / kBlock2, p.nx);
     launch_step_kernel(k_2d_e<T, EXACT>, grd, blk, 0, st, p, s);
@@ -1163,12 +1187,11 @@ template <typename T, bool EXACT> int profile_t(oidt_ctx *ctx, Job *J, int nstep
     }
     Params<T> &p = cells<T>(J)[par];
     if (J->d.mode == OIDT_MODE_YEE3D) {
-      dim3 blk(kBlock3Z, kBlock3Y), grd((p.nz + kBlock3Z - 1) / kBlock3Z, (p.ny + kBlock3Y - 1) / kBlock3Y, p.nx);
       cudaEventRecord(ev[q++], st);
-      k_y3_e<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+      y3_half<T, EXACT>(J->pl.rows, false, false, p, s, st);
       cudaEventRecord(ev[q++], st);
       cudaEventRecord(ev[q++], st);
-      k_y3_h<T, EXACT><<<grd, blk, 0, st>>>(p, s);
+      y3_half<T, EXACT>(J->pl.rows, true, false, p, s, st);
       cudaEventRecord(ev[q++], st);
       if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par, st);  // untimed
     } else {

@@ -88,14 +88,17 @@ VARIANTS = {"cell": 0, "sweep": 1}
 
 
 def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "cell",
-            graphs: bool = True):
+            graphs: bool = True, rows: int = 0, march_depth: int = 0):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
     ``keepalive`` must outlive the ``oidt_job_create`` call.
 
     ``variant`` (3D only): 'cell' (default) -- the per-cell E-half / H-half
     launches; 'sweep' -- one plane-sweep launch per step (E and H fused,
     TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
-    launches every step directly instead of replaying K-step CUDA graphs."""
+    launches every step directly instead of replaying K-step CUDA graphs.
+    ``rows`` (3D per-cell form): tile rows of a block, 2, 4 or 8 (0 = 4);
+    ``march_depth`` (3D plane sweep): x-planes per work item (0 = the
+    engine's makespan estimate).  ``oidt_b200.tune`` measures both."""
     prec = np.dtype(precision if precision is not None else spec.precision)
     if prec not in (np.dtype(np.float32), np.dtype(np.float64)):
         raise ValueError("precision must be float32 or float64")
@@ -143,6 +146,8 @@ def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int 
     d.ring_steps = ring_steps
     d.reserved[0] = VARIANTS[variant]
     d.reserved[1] = 0 if graphs else 1
+    d.reserved[2] = int(rows)
+    d.reserved[3] = int(march_depth)
     probe = spec.meta.get("probe")  # (y, z) of a 3D line probe along x
     if probe is not None:
         d.probe[0], d.probe[1], d.probe[2] = 1, int(probe[0]), int(probe[1])

@@ -153,6 +153,36 @@ def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     job.release()
 
 
+@pytest.mark.parametrize("choice", [{"variant": "cell", "rows": 2}, {"variant": "cell", "rows": 8},
+                                    {"variant": "sweep", "march_depth": 1}, {"variant": "sweep", "march_depth": 3},
+                                    {"variant": "sweep", "march_depth": 500}])
+@pytest.mark.parametrize("name", ["yee3d_te", "yee3d_tm", "yee3d_wide", "yee3d_graded"])
+def test_launch_choices_equal_oracle(eng, name, choice):
+    """Every launch choice the tuner may pick (tile rows 2 and 8 with ragged
+    last tiles; march depths 1, 3 and one longer than the guide) computes
+    the oracle's fields, CPML state and DFTs bit for bit."""
+    spec = _random_cases()[name]()
+    rng = np.random.default_rng(sum(map(ord, name)) + 17)
+    s = oracle_from_spec(spec)
+    job = eng.submit(spec, arith="exact", precision=np.float64, ring_steps=6, **choice)
+    for f in R.field_names(spec.mode):
+        v = rng.standard_normal(spec.shape) * 1e-2
+        getattr(s, f)[...] = v
+        job.set_field(f, v)
+    job.advance(7).advance(14).sync(60000)
+    R.run(s, 21)
+    for f, arr in job.fields().items():
+        np.testing.assert_array_equal(arr, getattr(s, f), err_msg=f)
+    from oidt_b200.spec import PSI
+    for fname, axis in PSI[spec.mode]:
+        for side in (0, 1):
+            np.testing.assert_array_equal(job.psi(fname, axis, side), getattr(s, psi_key(fname, axis, side)))
+    for port in (0, 1):
+        for c in range(4):
+            np.testing.assert_array_equal(job.dft(port, c), R.dft_complex(s, port, c), err_msg="port %d comp %d" % (port, c))
+    job.release()
+
+
 def _s_forward(spec, dfts_inc, dfts_ref):
     from oidt_b200.sparams import forward_s
     return forward_s(spec, dfts_inc, dfts_ref)

@@ -1,0 +1,100 @@
+"""Launch choices and the tuner, without a device: the descriptor fields for
+tile rows and march depth are validated by the host planner, and the tuner
+picks the fastest measured choice, caches it per shape key and persists it."""
+import ctypes
+import json
+
+import numpy as np
+import pytest
+
+from oidt_b200 import tune
+from oidt_b200 import workloads as W
+
+
+def _bytes(lib, d):
+    b = ctypes.c_uint64()
+    return lib.oidt_job_bytes(ctypes.byref(d), ctypes.byref(b)), b.value
+
+
+def _strip(**kw):
+    args = dict(nx=20, ny=19, nz=40, P=4, src_gap=2, port_gap=3, steps=200, nf=2, core_x_nm=120, core_y_nm=160)
+    args.update(kw)
+    return W.strip3d(**args)
+
+
+def test_descriptor_launch_choices_validated_on_host():
+    from oidt_b200.engine import load_library
+    from oidt_b200.spec import to_desc
+    lib = load_library()
+    spec = _strip()
+    rc, base = _bytes(lib, to_desc(spec)[0])
+    assert rc == 0
+    for rows in (2, 4, 8):  # tile rows change launches, not memory
+        d, keep = to_desc(spec, rows=rows)
+        assert _bytes(lib, d) == (0, base)
+    for rows in (1, 3, 16, -2):
+        d, keep = to_desc(spec, rows=rows)
+        assert _bytes(lib, d)[0] == -1, rows
+    d, keep = to_desc(spec, variant="sweep", rows=4)  # rows belong to the per-cell form
+    assert _bytes(lib, d)[0] == -1
+    d, keep = to_desc(spec, march_depth=8)  # march depth belongs to the plane sweep
+    assert _bytes(lib, d)[0] == -1
+    for depth in (1, 8, 10_000):
+        d, keep = to_desc(spec, variant="sweep", march_depth=depth)
+        assert _bytes(lib, d)[0] == 0, depth
+    d, keep = to_desc(spec, variant="sweep", march_depth=-1)
+    assert _bytes(lib, d)[0] == -1
+    slab = W.slab2d(nx=60, ny=50, P=5, core_cells=6, src_x=10, ports=(15, 45), steps=10, nf=3)
+    d, keep = to_desc(slab, rows=2)  # 2D has one launch form
+    assert _bytes(lib, d)[0] == -1
+    d, keep = to_desc(slab)
+    d.reserved[0] = 2  # no such launch form
+    assert _bytes(lib, d)[0] == -1
+
+
+class _FakeTuner(tune.Tuner):
+    """Timings from a table instead of the device."""
+
+    def __init__(self, table, **kw):
+        super().__init__(eng=None, **kw)
+        self.fake = table
+        self.calls = []
+
+    def time_choice(self, spec, choice, precision=None, arith="fast", ring_steps=32):
+        self.calls.append((spec.shape, tune.label(choice)))
+        return self.fake[tune.label(choice)]
+
+
+TIMES = {"cell/rows4": 0.090, "cell/rows2": 0.093, "cell/rows8": 0.088, "sweep/depth-auto": 0.140,
+         "sweep/depth16": 0.150}
+
+
+def test_tuner_picks_fastest_and_caches_per_shape(tmp_path):
+    path = str(tmp_path / "tune.json")
+    t = _FakeTuner(TIMES, cache_path=path)
+    a = _strip(nz=150)
+    c = t.choose(a, np.float32)
+    assert c == {"variant": "cell", "rows": 8, "march_depth": 0}
+    assert len(t.calls) == len(tune.CANDIDATES)
+    t.choose(_strip(nz=170), np.float32)  # same cross-section, guide length in the same 64-cell class
+    assert len(t.calls) == len(tune.CANDIDATES)
+    t.choose(_strip(nz=200), np.float32)  # next class: measured again
+    assert len(t.calls) == 2 * len(tune.CANDIDATES)
+    t.choose(a, np.float64)  # precision is part of the key
+    assert len(t.calls) == 3 * len(tune.CANDIDATES)
+    slab = W.slab2d(nx=60, ny=50, P=5, core_cells=6, src_x=10, ports=(15, 45), steps=10, nf=3)
+    assert t.choose(slab) == tune.DEFAULT and len(t.calls) == 3 * len(tune.CANDIDATES)
+    saved = json.load(open(path))
+    assert len(saved) == 3
+    # a new tuner reads the file and measures nothing for known shapes
+    t2 = _FakeTuner({k: 1.0 for k in TIMES}, cache_path=path)
+    assert t2.choose(a, np.float32) == c and t2.calls == []
+    s = t2.summary()
+    key = tune.shape_key(a, np.float32, "fast", 32)
+    assert s[key]["choice"] == "cell/rows8" and s[key]["default_ms_per_step"] == TIMES["cell/rows4"]
+
+
+def test_tuning_needs_enough_steps():
+    t = tune.Tuner(eng=None, reps=3)
+    with pytest.raises(ValueError):
+        t.time_choice(_strip(steps=100), dict(tune.DEFAULT), np.float32, ring_steps=32)
