@@ -31,7 +31,8 @@
 extern "C" {
 #endif
 
-#define OIDT_ABI_VERSION 2  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe) */
+#define OIDT_ABI_VERSION 3  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe);
+                              3: launch choices (reserved[2..3]), oidt_job_port_power */
 
 /* status codes */
 #define OIDT_OK 0
@@ -171,6 +172,25 @@ int32_t oidt_job_read_dft(oidt_ctx *ctx, uint64_t job, int32_t port, int32_t com
  * [nt, nx] recordings (FDTD/GPU/FDTD_3D/wave_impedance/fdtd_main.py:341-346).
  * OIDT_ERR_STATE if the job has no probe. */
 int32_t oidt_job_read_probe(oidt_ctx *ctx, uint64_t job, int32_t comp, void *out, size_t nbytes);
+
+/* Complex power through one port's plane, summed over a window on the
+ * device in float64: out[f] = sum over the window of the Poynting density
+ * 3D 1/2 (Ex Hy* - Ey Hx*), 2D TM -1/2 Ez Hy*, 2D TE 1/2 Ey Hz*, of this
+ * job's port DFT, or, with minus_job != 0, of this job's minus minus_job's
+ * at the same port (the reflected wave: device-under-test run minus
+ * incident run; same mode, nf and port plane required).  These are the sums
+ * S_ij = sqrt(P_ref / P_inc) is formed from (FDTD/GPU/FDTD_2D_TM/
+ * s-parameter_extraction/extract_sparams.py:88-104, FDTD_3D/.../
+ * extract_sparams.py:114-131, which sum over the window on the host after
+ * the [nf, plane] arrays were saved and loaded); here only nf complex
+ * values cross the link.  window = {i0, i1, j0, j1}: rows [i0, i1) x columns [j0, j1)
+ * of the port plane, 3D [nx][ny], 2D one row of ny (i0 = 0, i1 = 1).
+ * out = nf complex128 (re, im interleaved; n_doubles >= 2 nf).  Waits for
+ * the steps enqueued on both jobs, on a stream of its own.  The summation
+ * order is fixed (block tree per frequency), so results are deterministic;
+ * they equal the host sums up to float64 rounding. */
+int32_t oidt_job_port_power(oidt_ctx *ctx, uint64_t job, uint64_t minus_job, int32_t port,
+                            const int32_t window[4], double *out_re_im, size_t n_doubles);
 
 /* Port-window DFT of one (port, comp), as oidt_job_read_dft but restricted
  * to the DFT window [win_lo, win_hi): out = complex128 [nf][wi][wj] (3D, wi =

@@ -15,7 +15,9 @@ source, not on the roughness or the guide length, so:
   K-step blocks replayed from a CUDA graph).
 
 Both take an optional :class:`oidt_b200.tune.Tuner`; each job is then launched
-with the choices measured for its shape (results are unchanged by them).
+with the choices measured for its shape (results are unchanged by them).  Both
+sum the S-parameter powers on the device (``forward_s_device``): the DFT planes
+stay in HBM and only 3 x nf complex values per realization are read back.
 """
 from __future__ import annotations
 
@@ -25,7 +27,7 @@ import numpy as np
 
 from . import workloads as W
 from .engine import Engine
-from .sparams import forward_s
+from .sparams import forward_s_device
 
 
 def incident_length(kw: dict) -> int:
@@ -49,10 +51,6 @@ def realization_set(configs, nf=41, precision=np.float32, **common):
             incidents[key] = W.strip3d(**dict(kw, rough=False, nz=incident_length(kw)))
         keys.append(key)
     return roughs, keys, incidents
-
-
-def _dfts(job):
-    return {(p, c): job.dft(p, c) for p in (0, 1) for c in range(4)}
 
 
 def _choice(tuner, spec, precision, ring_steps):
@@ -83,8 +81,8 @@ def run_batched(eng: Engine, rset, precision=np.float32, ring_steps=32, tuner=No
             j.advance(j.spec.nt - steps)
     for j in jobs:
         j.sync()
-    inc = {k: _dfts(jobs[len(roughs) + n]) for n, k in enumerate(inc_keys)}
-    res = [forward_s(roughs[r], inc[keys[r]], _dfts(jobs[r])) for r in range(len(roughs))]
+    inc = {k: jobs[len(roughs) + n] for n, k in enumerate(inc_keys)}
+    res = [forward_s_device(roughs[r], inc[keys[r]], jobs[r]) for r in range(len(roughs))]
     for j in jobs:
         j.release()
     return time.perf_counter() - t0, res
@@ -102,7 +100,7 @@ def run_plain(eng: Engine, rset, precision=np.float32, tuner=None):
         ji = eng.submit(incidents[key], precision=precision, graphs=False,
                         **_choice(tuner, incidents[key], precision, 32))
         ji.run().sync()
-        res.append(forward_s(spec_r, _dfts(ji), _dfts(jr)))
+        res.append(forward_s_device(spec_r, ji, jr))
         jr.release()
         ji.release()
     return time.perf_counter() - t0, res

@@ -467,6 +467,7 @@ struct JobPlan {
   size_t off_psi[2][6][3][2];
   size_t off_jsrc, off_tw[4], off_ring, off_acc, off_state, off_tmaps, off_items;
   size_t off_probe, probe_bytes;  // line probe [4][nt][nx] (probe_bytes = 0: none)
+  size_t off_pow;                 // port power [nf] complex float64
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
   int rows;  // 3D per-cell tile rows
@@ -633,6 +634,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->off_ring = L.take((size_t)K * 2 * nslot_of(d->mode) * plane * esz);
   pl->off_acc = L.take((size_t)2 * ncomp_of(d->mode) * d->nf * plane * 16);
   pl->off_state = L.take(64);
+  pl->off_pow = L.take((size_t)d->nf * 16);
   if (d->probe[0] == 1) {
     pl->probe_bytes = (size_t)4 * d->nt * d->nx * esz;
     pl->off_probe = L.take(pl->probe_bytes);
@@ -696,6 +698,7 @@ struct oidt_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;  // compute
   cudaStream_t upload = nullptr;  // job creation copies
+  cudaStream_t readout = nullptr; // port-power reductions (never queued behind compute)
   cudaStream_t aux[kAuxStreams] = {};  // branches of multi-job blocks
   cudaEvent_t fork = nullptr, join[kAuxStreams] = {};
   uint64_t budget = 0, in_use = 0;
@@ -1300,7 +1303,8 @@ int32_t oidt_create(int32_t device, uint64_t hbm_budget, oidt_ctx **out) {
   oidt_ctx *ctx = new oidt_ctx();
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->upload, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&ctx->upload, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->readout, cudaStreamNonBlocking) != cudaSuccess) {
     delete ctx;
     return OIDT_ERR_CUDA;
   }
@@ -1333,8 +1337,10 @@ int32_t oidt_destroy(oidt_ctx *ctx) {
       cudaEventDestroy(ctx->join[a]);
     }
     cudaEventDestroy(ctx->fork);
+    cudaStreamSynchronize(ctx->readout);
     cudaStreamDestroy(ctx->stream);
     cudaStreamDestroy(ctx->upload);
+    cudaStreamDestroy(ctx->readout);
   }
   delete ctx;
   return OIDT_OK;
@@ -1511,6 +1517,122 @@ int32_t oidt_job_read_probe(oidt_ctx *ctx, uint64_t job, int32_t comp, void *out
   int rc = read_common(ctx, J);
   if (rc) return rc;
   CU(ctx, cudaMemcpy(out, J->mem + J->pl.off_probe + comp * need, need, cudaMemcpyDeviceToHost));
+  return OIDT_OK;
+}
+
+// ---- port power: the S-parameter sums, reduced on the device ----------------
+// P[f] = sum over the window of the port plane's complex Poynting density in
+// float64: 3D 1/2 (Ex Hy* - Ey Hx*) (FDTD_3D extract_sparams.py:114-115), 2D TM
+// -1/2 Ez Hy*, 2D TE 1/2 Ey Hz* (FDTD_2D_TM / FDTD_2D_TE extract_sparams.py:
+// 88-89), of this job's accumulators or of their difference with another
+// job's (the reflected wave).  One block per frequency; each thread sums a
+// strided subset of the window, then a fixed-shape tree combines the
+// threads, so the result does not depend on scheduling.
+namespace {
+constexpr int kPowThreads = 256;
+struct PowerArgs {
+  const double2 *a[4], *b[4];  // b[0] == nullptr: no subtraction
+  double2 *out;
+  long long plane;
+  int cols, i0, j0, wi, wj, mode;
+};
+
+__device__ __forceinline__ double2 cmul_conj(double2 u, double2 v) {  // u * conj(v)
+  return make_double2(u.x * v.x + u.y * v.y, u.y * v.x - u.x * v.y);
+}
+
+__global__ void __launch_bounds__(kPowThreads) k_port_power(PowerArgs a) {
+  const int f = blockIdx.x;
+  const long long n = (long long)a.wi * a.wj, base = (long long)f * a.plane;
+  const int nc = a.mode == OIDT_MODE_YEE3D ? 4 : 2;
+  double re = 0.0, im = 0.0;
+  for (long long t = threadIdx.x; t < n; t += kPowThreads) {
+    const long long o = base + (long long)(a.i0 + (int)(t / a.wj)) * a.cols + (a.j0 + (int)(t % a.wj));
+    double2 v[4];
+    for (int c = 0; c < nc; ++c) {
+      v[c] = a.a[c][o];
+      if (a.b[0]) {
+        const double2 w = a.b[c][o];
+        v[c].x -= w.x;
+        v[c].y -= w.y;
+      }
+    }
+    double2 p;
+    if (a.mode == OIDT_MODE_YEE3D) {
+      const double2 p1 = cmul_conj(v[0], v[3]), p2 = cmul_conj(v[1], v[2]);
+      p = make_double2(0.5 * (p1.x - p2.x), 0.5 * (p1.y - p2.y));
+    } else {
+      const double2 q = cmul_conj(v[0], v[1]);
+      const double s = a.mode == OIDT_MODE_TM2 ? -0.5 : 0.5;
+      p = make_double2(s * q.x, s * q.y);
+    }
+    re += p.x;
+    im += p.y;
+  }
+  for (int d = 16; d > 0; d >>= 1) {
+    re += __shfl_down_sync(0xffffffffu, re, d);
+    im += __shfl_down_sync(0xffffffffu, im, d);
+  }
+  __shared__ double sr[kPowThreads / 32], si[kPowThreads / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { sr[w] = re; si[w] = im; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0, i = 0.0;
+    for (int q = 0; q < kPowThreads / 32; ++q) { r += sr[q]; i += si[q]; }
+    a.out[f] = make_double2(r, i);
+  }
+}
+}  // namespace
+
+int32_t oidt_job_port_power(oidt_ctx *ctx, uint64_t job, uint64_t minus_job, int32_t port, const int32_t *window,
+                            double *out, size_t n) {
+  if (!ctx || !out || !window) return OIDT_ERR_INVALID;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  Job *J = find(ctx, job);
+  if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
+  Job *M = nullptr;
+  if (minus_job) {
+    M = find(ctx, minus_job);
+    if (!M) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)minus_job);
+    if (M == J) return fail(ctx, OIDT_ERR_INVALID, "minus_job is the job itself");
+    // the port plane: 3D [nx][ny], 2D [ny] (nx is then the guide length, free)
+    if (M->d.mode != J->d.mode || M->d.nf != J->d.nf || M->d.ny != J->d.ny ||
+        (J->d.mode == OIDT_MODE_YEE3D && M->d.nx != J->d.nx))
+      return fail(ctx, OIDT_ERR_INVALID, "minus_job needs the same mode, nf and port plane");
+  }
+  if (port < 0 || port > 1) return fail(ctx, OIDT_ERR_INVALID, "bad port");
+  const bool is3 = J->d.mode == OIDT_MODE_YEE3D;
+  const int rows = is3 ? J->d.nx : 1, cols = J->d.ny;
+  const int i0 = window[0], i1 = window[1], j0 = window[2], j1 = window[3];
+  if (i0 < 0 || i1 > rows || i0 >= i1 || j0 < 0 || j1 > cols || j0 >= j1)
+    return fail(ctx, OIDT_ERR_INVALID, "window must lie in the %d x %d port plane and be non-empty", rows, cols);
+  if (n < (size_t)2 * J->d.nf) return fail(ctx, OIDT_ERR_INVALID, "output needs %d doubles", 2 * J->d.nf);
+  CU(ctx, cudaSetDevice(ctx->device));
+  for (Job *X : {J, M}) {  // uploaded, and every step enqueued so far done
+    if (!X) continue;
+    CU(ctx, cudaStreamWaitEvent(ctx->readout, X->ready, 0));
+    CU(ctx, cudaStreamWaitEvent(ctx->readout, X->done, 0));
+  }
+  const int nc = ncomp_of(J->d.mode);
+  const size_t span = (size_t)J->d.nf * J->pl.plane;
+  PowerArgs a = {};
+  for (int c = 0; c < nc; ++c) {
+    a.a[c] = reinterpret_cast<const double2 *>(J->mem + J->pl.off_acc) + ((size_t)port * nc + c) * span;
+    if (M) a.b[c] = reinterpret_cast<const double2 *>(M->mem + M->pl.off_acc) + ((size_t)port * nc + c) * span;
+  }
+  a.out = reinterpret_cast<double2 *>(J->mem + J->pl.off_pow);
+  a.plane = J->pl.plane;
+  a.cols = cols;
+  a.i0 = i0;
+  a.j0 = j0;
+  a.wi = i1 - i0;
+  a.wj = j1 - j0;
+  a.mode = J->d.mode;
+  k_port_power<<<J->d.nf, kPowThreads, 0, ctx->readout>>>(a);
+  CU(ctx, cudaGetLastError());
+  CU(ctx, cudaMemcpyAsync(out, a.out, (size_t)J->d.nf * 16, cudaMemcpyDeviceToHost, ctx->readout));
+  CU(ctx, cudaStreamSynchronize(ctx->readout));
   return OIDT_OK;
 }
 

@@ -22,7 +22,7 @@ EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error",
            "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
            "oidt_job_query", "oidt_job_read_dft", "oidt_job_read_field", "oidt_job_write_field",
            "oidt_job_read_psi", "oidt_job_release", "oidt_job_reset", "oidt_ctx_stream", "oidt_job_profile",
-           "oidt_job_read_dft_window_static", "oidt_job_read_probe")
+           "oidt_job_read_dft_window_static", "oidt_job_read_probe", "oidt_job_port_power")
 
 
 class OidtError(RuntimeError):
@@ -73,6 +73,7 @@ def load_library(path: str = LIB_PATH):
             "oidt_job_read_dft": ([vp, u64, i32, i32, vp, C.c_size_t], i32),
             "oidt_job_read_dft_window_static": ([vp, u64, i32, i32, vp, C.c_size_t], i32),
             "oidt_job_read_probe": ([vp, u64, i32, vp, C.c_size_t], i32),
+            "oidt_job_port_power": ([vp, u64, u64, i32, C.POINTER(i32), vp, C.c_size_t], i32),
             "oidt_job_read_field": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_write_field": ([vp, u64, i32, vp, C.c_size_t], i32),
             "oidt_job_read_psi": ([vp, u64, i32, i32, i32, vp, C.c_size_t], i32),
@@ -219,6 +220,24 @@ class Job:
         out = np.empty((self.spec.nf,) + win, dtype=np.complex128)
         self.eng._check(self.eng.lib.oidt_job_read_dft_window_static(self.eng.ctx, self.id, port, ci,
                                                                      out.ctypes.data, out.size * 2))
+        return out
+
+    def port_power(self, port: int, minus: "Job" = None, window=None) -> np.ndarray:
+        """complex128 [nf]: the port plane's Poynting flux summed over
+        ``window`` on the device in float64 (``oidt_job_port_power``).
+        ``minus``: a job whose DFT at the same port is subtracted first (the
+        reflected wave).  ``window`` defaults to the spec's power window:
+        3D ((i0, i1), (j0, j1)) over [nx][ny], 2D (j0, j1) over ny."""
+        from .spec import power_window
+        w = power_window(self.spec) if window is None else window
+        if self.spec.mode == "yee3d":
+            (i0, i1), (j0, j1) = w
+        else:
+            (i0, i1), (j0, j1) = (0, 1), w
+        win = (C.c_int32 * 4)(int(i0), int(i1), int(j0), int(j1))
+        out = np.empty(self.spec.nf, dtype=np.complex128)
+        self.eng._check(self.eng.lib.oidt_job_port_power(self.eng.ctx, self.id, minus.id if minus is not None else 0,
+                                                         port, win, out.ctypes.data, out.size * 2))
         return out
 
     PROBE_COMPS = ("ey", "ez", "hy", "hz")

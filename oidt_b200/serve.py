@@ -28,7 +28,7 @@ import numpy as np
 
 from . import workloads as W
 from .engine import BudgetError, Engine
-from .sparams import forward_s
+from .sparams import forward_s_device
 
 
 @dataclass
@@ -89,15 +89,15 @@ class Server:
         return True
 
     def _finish(self, entry, t0: float):
-        """Read the DFTs of a completed request, compute S, free its jobs."""
+        """S of a completed request from its port powers, summed on the device
+        (its DFT planes are read back only with ``keep_dfts``); free its jobs."""
         req, j, ji, adm = entry
         jobs = [x for x in (j, ji) if x is not None]
         for x in jobs:
             x.sync()
         nc = 4 if req.spec.mode == "yee3d" else 2
-        d_ref = {(p, c): j.dft(p, c) for p in (0, 1) for c in range(nc)}
-        d_inc = {(p, c): ji.dft(p, c) for p in (0, 1) for c in range(nc)} if ji is not None else d_ref
-        S = forward_s(req.spec, d_inc, d_ref)
+        S = forward_s_device(req.spec, ji if ji is not None else j, j)
+        d_ref = {(p, c): j.dft(p, c) for p in (0, 1) for c in range(nc)} if self.keep_dfts else None
         fin = time.perf_counter() - t0
         self.results.append(Result(req.rid, req.arrival, adm, fin, req.spec.ncells, req.spec.nt,
                                    S={k: v for k, v in S.items() if k != "P_inc"},

@@ -4,7 +4,8 @@
   extraction (``FDTD_2D_TM/.../extract_sparams.py:48-104``,
   ``FDTD_3D/.../extract_sparams.py:48-131``) on the saved DFT arrays.
 * :func:`forward_s` -- S11 / S21 from one incident and one reflected run
-  (the two runs the forward protocol needs), summed over a power window.
+  (the two runs the forward protocol needs), summed over a power window;
+  :func:`forward_s_device` -- the same with the sums reduced on the device.
 * :func:`write_touchstone` / :func:`read_touchstone` -- RI-format ``.sNp`` in
   the layout the reference's scikit-rf 0.18 writer produces
   (``extract_sparams.py:106-117``), with the OIDT comment line first.
@@ -16,6 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 from .refsetup import derive
+from .spec import power_window
 
 OIDT_ACK = ("!This S-parameter file was generated as part of the OIDT. This project was completed as part of "
             "research conducted with my major professor and advisor, Prof. Ata Zadehgol, at the Applied and "
@@ -37,11 +39,11 @@ def power_density(mode: str, comps):
 
 
 def _window_power(spec, sav):
-    w = spec.meta.get("power_window")
+    w = power_window(spec)
     if spec.mode == "yee3d":
-        (i0, i1), (j0, j1) = w if w else ((spec.win_lo[0], spec.win_hi[0]), (spec.win_lo[1], spec.win_hi[1]))
+        (i0, i1), (j0, j1) = w
         return sav[:, i0:i1, j0:j1].sum(axis=(1, 2))
-    j0, j1 = w if w else (spec.win_lo[1], spec.win_hi[1])
+    j0, j1 = w
     return sav[:, j0:j1].sum(axis=1)
 
 
@@ -57,6 +59,19 @@ def forward_s(spec, inc: dict, ref: dict) -> dict:
     p_inc = _window_power(spec, power_density(spec.mode, a1))
     p_ref = _window_power(spec, power_density(spec.mode, r1))
     p_tr = _window_power(spec, power_density(spec.mode, t2))
+    return {"S11": np.sqrt(p_ref / p_inc), "S21": np.sqrt(p_tr / p_inc), "P_inc": p_inc}
+
+
+def forward_s_device(spec, inc_job, ref_job) -> dict:
+    """:func:`forward_s` with its three power sums reduced on the device
+    (``Job.port_power``, float64): the DFT planes stay in HBM and 3 x nf
+    complex values cross the link.  ``inc_job`` may be ``ref_job`` itself
+    (no separate incident run), as ``forward_s(spec, d, d)`` allows: the
+    reflected power is then 0."""
+    w = power_window(spec)
+    p_inc = inc_job.port_power(0, window=w)
+    p_ref = np.zeros_like(p_inc) if inc_job is ref_job else ref_job.port_power(0, minus=inc_job, window=w)
+    p_tr = ref_job.port_power(1, window=w)
     return {"S11": np.sqrt(p_ref / p_inc), "S21": np.sqrt(p_tr / p_inc), "P_inc": p_inc}
 
 

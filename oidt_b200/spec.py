@@ -87,6 +87,16 @@ class JobDesc(C.Structure):
 VARIANTS = {"cell": 0, "sweep": 1}
 
 
+def power_window(spec: SimSpec):
+    """The window S-parameter powers are summed over: ``meta['power_window']``
+    if set, else the DFT window.  3D ((i0, i1), (j0, j1)) over the [nx][ny]
+    port plane; 2D (j0, j1) over its ny cells."""
+    w = spec.meta.get("power_window")
+    if spec.mode == "yee3d":
+        return tuple(map(tuple, w)) if w else ((spec.win_lo[0], spec.win_hi[0]), (spec.win_lo[1], spec.win_hi[1]))
+    return tuple(w) if w else (spec.win_lo[1], spec.win_hi[1])
+
+
 def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "cell",
             graphs: bool = True, rows: int = 0, march_depth: int = 0):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in

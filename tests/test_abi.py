@@ -30,7 +30,7 @@ def test_library_exports_all_declared_symbols():
     assert set(EXPORTS) <= set(declared())
     f = lib.oidt_abi_version
     f.restype = ctypes.c_int32
-    assert f() == 2
+    assert f() == 3
 
 
 def test_descriptor_validation_without_device():

@@ -33,6 +33,9 @@ class FakeJob:
     def dft(self, port, comp):
         return np.ones((self.spec.nf, self.spec.shape[1]), complex) * (1 + port)
 
+    def port_power(self, port, minus=None, window=None):
+        return np.full(self.spec.nf, 0.0 if minus is not None else 1.0 + port, complex)
+
     def release(self):
         self.released = True
         self.eng.in_use -= self.spec.bytes
