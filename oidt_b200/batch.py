@@ -88,17 +88,18 @@ def run_batched(eng: Engine, rset, precision=np.float32, ring_steps=32, tuner=No
     return time.perf_counter() - t0, res
 
 
-def run_plain(eng: Engine, rset, precision=np.float32, tuner=None):
+def run_plain(eng: Engine, rset, precision=np.float32, tuner=None, ring_steps=32):
     """One run at a time, launched step by step: each realization's rough
     run, then its own incident run."""
     roughs, keys, incidents = rset
     t0 = time.perf_counter()
     res = []
     for spec_r, key in zip(roughs, keys):
-        jr = eng.submit(spec_r, precision=precision, graphs=False, **_choice(tuner, spec_r, precision, 32))
+        jr = eng.submit(spec_r, precision=precision, graphs=False, ring_steps=ring_steps,
+                        **_choice(tuner, spec_r, precision, ring_steps))
         jr.run().sync()
-        ji = eng.submit(incidents[key], precision=precision, graphs=False,
-                        **_choice(tuner, incidents[key], precision, 32))
+        ji = eng.submit(incidents[key], precision=precision, graphs=False, ring_steps=ring_steps,
+                        **_choice(tuner, incidents[key], precision, ring_steps))
         ji.run().sync()
         res.append(forward_s_device(spec_r, ji, jr))
         jr.release()
@@ -111,7 +112,7 @@ def s21_loss_db(results):
     return np.array([float(np.mean(-20 * np.log10(np.abs(r["S21"])))) for r in results])
 
 
-def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0, tuned=True):
+def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0, tuned=True, ring_steps=32):
     """Realizations/s of the batched path against the plain one-run-at-a-time
     path on ``n`` realizations drawn like the batched stochastic set (uneven
     grids), and the largest |S21 difference| between the two (the same
@@ -128,13 +129,14 @@ def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0, tuned=True):
         from .tune import Tuner
         tuner = Tuner(eng)
         t0 = time.perf_counter()
-        tune_set(tuner, rset)
+        tune_set(tuner, rset, ring_steps=ring_steps)
         t_tune = time.perf_counter() - t0
-    t_plain, s_plain = run_plain(eng, rset, tuner=tuner)
-    t_batch, s_batch = run_batched(eng, rset, tuner=tuner)
+    t_plain, s_plain = run_plain(eng, rset, tuner=tuner, ring_steps=ring_steps)
+    t_batch, s_batch = run_batched(eng, rset, ring_steps=ring_steps, tuner=tuner)
     d = max(float(np.max(np.abs(a["S21"] - b["S21"]))) for a, b in zip(s_plain, s_batch))
     loss = s21_loss_db(s_batch)
-    return {"realizations": n, "steps": steps, "nf": nf, "shared_incident_runs": len(incidents),
+    return {"realizations": n, "steps": steps, "nf": nf, "ring_steps": ring_steps,
+            "shared_incident_runs": len(incidents),
             "plain_cell_updates": int(plain_cells), "batched_cell_updates": int(batched_cells),
             "plain_s": round(t_plain, 3), "batched_s": round(t_batch, 3),
             "plain_realizations_per_s": round(n / t_plain, 3), "batched_realizations_per_s": round(n / t_batch, 3),
@@ -142,14 +144,14 @@ def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0, tuned=True):
             "s21_loss_db_mean": float(np.mean(loss)), "s21_loss_db_std": float(np.std(loss)),
             "launch_tuning": None if tuner is None else {
                 "seconds": round(t_tune, 3), "shapes": len(tuner.table),
-                "choices": _histogram(tuner, rset)}}
+                "choices": _histogram(tuner, rset, ring_steps=ring_steps)}}
 
 
-def _histogram(tuner, rset, precision=np.float32):
+def _histogram(tuner, rset, precision=np.float32, ring_steps=32):
     from .tune import label
     roughs, keys, incidents = rset
     h = {}
     for s in list(roughs) + list(incidents.values()):
-        c = label(tuner.choose(s, precision))
+        c = label(tuner.choose(s, precision, ring_steps=ring_steps))
         h[c] = h.get(c, 0) + 1
     return h

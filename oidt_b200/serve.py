@@ -13,8 +13,8 @@ Requests (a SimSpec each, or a builder for one) arrive over time.  The loop
    tick, so a small job (a 2D run beside 3D ones) leaves after a tick or two
    instead of queuing behind the large jobs' steps; total work and every
    result are unchanged (``fair_share=False`` gives every job ``tick`` steps);
-3. retires finished jobs: reads their port DFTs, computes S11/S21, records
-   latency = finish time - arrival time, frees their memory.
+3. retires finished jobs: sums their port powers on the device, forms
+   S11/S21, records latency = finish time - arrival time, frees their memory.
 
 So requests that arrive while others are on the GPU join at the next tick
 and share launches with them; nothing waits for a batch to drain.
@@ -210,17 +210,18 @@ def requests_from_mix(mix, nf=21, precision=np.float32):
     return out
 
 
-def measure(eng: Engine, rate_hz=20.0, duration_s=3.0, seed=0, tick=64, max_wall=300.0, warmup=True):
+def measure(eng: Engine, rate_hz=20.0, duration_s=3.0, seed=0, tick=64, max_wall=300.0, warmup=True,
+            ring_steps=32):
     """Serve the first ``duration_s`` seconds of the served mix at ``rate_hz``
     with arrivals honoured on the wall clock; latency and throughput.  A
     server pays its start-up once (kernel module loads, the first graph
     instantiations, device memory pool growth); with ``warmup`` the same
     length of the mix with another seed is served first, untimed."""
     if warmup:
-        Server(eng, tick=tick).run(requests_from_mix(W.serving_mix(rate_hz=rate_hz, duration_s=duration_s,
+        Server(eng, tick=tick, ring_steps=ring_steps).run(requests_from_mix(W.serving_mix(rate_hz=rate_hz, duration_s=duration_s,
                                                                    seed=seed + 1)), realtime=True, max_wall=max_wall)
     reqs = requests_from_mix(W.serving_mix(rate_hz=rate_hz, duration_s=duration_s, seed=seed))
-    srv = Server(eng, tick=tick)
+    srv = Server(eng, tick=tick, ring_steps=ring_steps)
     t0 = time.perf_counter()
     res = srv.run(reqs, realtime=True, max_wall=max_wall)
     wall = time.perf_counter() - t0
