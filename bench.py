@@ -342,12 +342,15 @@ def run_engine(args, ws, rank, local):
     e2e = dist_max(dist, float(np.mean(e2e_ms)), local)
     e2e_value = whole_job_rate(ws, spec.ncells, spec.nt, e2e)
 
-    # ---- batched realizations and the served mix (rank 0) ----------------
+    # ---- batched realizations and the served mix (one GPU: at N > 1 they
+    # would hold every GPU while rank 0 alone works) -------------------------
     batched = serving = slab2d = None
-    if rank == 0 and not args.no_extra:
+    if rank == 0 and ws == 1 and not args.no_extra:
         from oidt_b200 import batch as B, serve as SV
-        batched = B.measure(eng, n=args.batch_n, steps=3000)
+        # serving first: its latencies then see no host state left by the
+        # batched leg's 64 realization specs
         serving = SV.measure(eng, rate_hz=20.0, duration_s=args.serve_window)
+        batched = B.measure(eng, n=args.batch_n, steps=3000)
         slab2d = measure_slab2d(eng)
 
     cpu = None
@@ -396,7 +399,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the batched-realization, served-mix and 2D slab measurements")
-    ap.add_argument("--batch-n", type=int, default=16, help="realizations in the batched-vs-plain measurement")
+    ap.add_argument("--batch-n", type=int, default=64, help="realizations in the batched-vs-plain measurement")
     ap.add_argument("--serve-window", type=float, default=3.0, help="seconds of served-mix arrivals (20 jobs/s)")
     args = ap.parse_args()
     ws, rank, local = dist_env()

@@ -142,6 +142,7 @@ def measure(eng: Engine, n=16, steps=3000, nf=41, master_seed=0, tuned=True, rin
             "plain_realizations_per_s": round(n / t_plain, 3), "batched_realizations_per_s": round(n / t_batch, 3),
             "speedup": round(t_plain / t_batch, 3), "max_abs_dS21_batched_vs_plain": d,
             "s21_loss_db_mean": float(np.mean(loss)), "s21_loss_db_std": float(np.std(loss)),
+            "s21_loss_db_percentiles": {str(q): float(np.percentile(loss, q)) for q in (0, 5, 25, 50, 75, 95, 100)},
             "launch_tuning": None if tuner is None else {
                 "seconds": round(t_tune, 3), "shapes": len(tuner.table),
                 "choices": _histogram(tuner, rset, ring_steps=ring_steps)}}
