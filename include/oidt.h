@@ -148,9 +148,10 @@ int32_t oidt_job_advance(oidt_ctx *ctx, uint64_t job, int32_t nsteps);
 
 /* Advance several jobs together (they may differ in size and solver; they
  * must share ring_steps): every ring block of steps forks one branch per job
- * onto auxiliary streams, so independent jobs run concurrently, and the block
- * is captured once per composition (jobs and their buffer parities) into a
- * CUDA graph that later calls replay; a context keeps eight compositions. */
+ * onto auxiliary streams, so independent jobs run concurrently.  A job's full
+ * ring block is its own CUDA graph (captured at its first full block, the
+ * graph oidt_job_advance replays), so a group whose membership changes from
+ * call to call costs no capture. */
 int32_t oidt_batch_advance(oidt_ctx *ctx, const uint64_t *jobs, int32_t njobs, int32_t nsteps);
 
 /* Bounded wait for the job's enqueued work.  timeout_ms < 0: no limit. */

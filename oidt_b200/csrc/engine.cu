@@ -677,19 +677,6 @@ struct Job {
   bool busy = false;
 };
 
-struct BatchPlan {  // cached multi-job composition: one CUDA graph per K-step block
-  std::vector<uint64_t> ids;
-  std::vector<int> pars;
-  cudaGraphExec_t graph = nullptr;
-  long long graph_launches = 0;
-  int K = 0;
-  unsigned long long last_use = 0;
-};
-// Compositions kept: a serving loop that advances its jobs in a few groups
-// (small jobs take more steps per tick than large ones) replays each group's
-// graph without re-capturing it while the group's membership is unchanged.
-constexpr int kBatchCache = 8;
-
 constexpr int kAuxStreams = 64;  // a served request is two jobs; the mix keeps ~40 active
 
 }  // namespace
@@ -707,8 +694,6 @@ struct oidt_ctx {
   std::mutex mu;
   std::string err;
   long long launches = 0;
-  BatchPlan batch[kBatchCache];
-  unsigned long long batch_clock = 0;
 };
 
 namespace {
@@ -1011,6 +996,26 @@ template <typename T, bool EXACT> void launch_fold(oidt_ctx *ctx, Job *J, int co
 
 int steps_flip(const Job *J) { return J->pl.variant == kVariantSweep ? 1 : 0; }
 
+// The job's K-step block starting on buffer parity par (its steps, then its
+// DFT fold) as a CUDA graph, captured on stream st at first use.  Capture
+// enqueues nothing, so st may hold work of other jobs.
+template <typename T, bool EXACT> int job_graph(oidt_ctx *ctx, Job *J, int par, cudaStream_t st) {
+  if (J->graph[par]) return OIDT_OK;
+  const int K = J->pl.K, flip = steps_flip(J);
+  cudaGraph_t g;
+  const long long before = ctx->launches;
+  CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  for (int s = 0; s < K; ++s) launch_step<T, EXACT>(ctx, J, s, par ^ (flip & s), st);
+  launch_fold<T, EXACT>(ctx, J, K, st);
+  CU(ctx, cudaStreamEndCapture(st, &g));
+  const cudaError_t ie = cudaGraphInstantiate(&J->graph[par], g, 0);
+  cudaGraphDestroy(g);
+  CU(ctx, ie);
+  J->graph_launches = ctx->launches - before;
+  ctx->launches = before;
+  return OIDT_OK;
+}
+
 template <typename T, bool EXACT> int advance_t(oidt_ctx *ctx, Job *J, int nsteps) {
   cudaStream_t st = ctx->stream;
   CU(ctx, cudaStreamWaitEvent(st, J->ready, 0));
@@ -1021,18 +1026,8 @@ template <typename T, bool EXACT> int advance_t(oidt_ctx *ctx, Job *J, int nstep
     const int cnt = std::min(K, left);
     const int par = J->parity;
     if (cnt == K && J->d.reserved[1] == 0) {
-      if (!J->graph[par]) {
-        cudaGraph_t g;
-        const long long before = ctx->launches;
-        CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        for (int s = 0; s < K; ++s) launch_step<T, EXACT>(ctx, J, s, par ^ (flip & s), st);
-        launch_fold<T, EXACT>(ctx, J, K, st);
-        CU(ctx, cudaStreamEndCapture(st, &g));
-        CU(ctx, cudaGraphInstantiate(&J->graph[par], g, 0));
-        CU(ctx, cudaGraphDestroy(g));
-        J->graph_launches = ctx->launches - before;
-        ctx->launches = before;
-      }
+      int rc = job_graph<T, EXACT>(ctx, J, par, st);
+      if (rc) return rc;
       CU(ctx, cudaGraphLaunch(J->graph[par], st));
       ctx->launches += J->graph_launches;
     } else {
@@ -1056,18 +1051,21 @@ int advance(oidt_ctx *ctx, Job *J, int nsteps) {
 }
 
 // ---- multi-job launches ----------------------------------------------------
-// A block of cnt steps for several jobs: each job's launches (its steps, then
-// its DFT fold) go to one of the auxiliary streams, forked from and joined
-// back into the compute stream, so independent jobs run concurrently and the
-// whole block is one CUDA graph when captured.
-void drop_batch(BatchPlan &bp) {
-  if (bp.graph) cudaGraphExecDestroy(bp.graph);
-  bp.graph = nullptr;
-  bp.ids.clear();
-  bp.pars.clear();
-}
-
+// A block of cnt steps for several jobs: each job's launches go to one of the
+// auxiliary streams, forked from and joined back into the compute stream, so
+// independent jobs run concurrently.  A full K-step block of a job is its own
+// CUDA graph (the graph single-job advances replay), so a group whose
+// membership changes from one call to the next -- a serving loop's groups do
+// at every admission and retirement -- costs no capture; launches of one
+// graph are ordered by CUDA even when they go to different streams.
 template <typename T, bool EXACT> int batch_block(oidt_ctx *ctx, std::vector<Job *> &js, int cnt, cudaStream_t st) {
+  const bool full = cnt == js[0]->pl.K;
+  if (full)  // capture missing graphs before the fork (capture enqueues nothing)
+    for (Job *J : js)
+      if (J->d.reserved[1] == 0) {
+        int rc = job_graph<T, EXACT>(ctx, J, J->parity, st);
+        if (rc) return rc;
+      }
   const int na = std::min<int>(kAuxStreams, (int)js.size());
   CU(ctx, cudaEventRecord(ctx->fork, st));
   for (int a = 0; a < na; ++a) CU(ctx, cudaStreamWaitEvent(ctx->aux[a], ctx->fork, 0));
@@ -1075,8 +1073,14 @@ template <typename T, bool EXACT> int batch_block(oidt_ctx *ctx, std::vector<Job
     Job *J = js[b];
     cudaStream_t sb = ctx->aux[b % na];
     const int flip = steps_flip(J);
-    for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, J->parity ^ (flip & s), sb);
-    launch_fold<T, EXACT>(ctx, J, cnt, sb);
+    if (full && J->d.reserved[1] == 0) {
+      CU(ctx, cudaGraphLaunch(J->graph[J->parity], sb));
+      ctx->launches += J->graph_launches;
+    } else {
+      for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, J->parity ^ (flip & s), sb);
+      launch_fold<T, EXACT>(ctx, J, cnt, sb);
+    }
+    J->parity ^= flip & cnt;
   }
   for (int a = 0; a < na; ++a) {
     CU(ctx, cudaEventRecord(ctx->join[a], ctx->aux[a]));
@@ -1093,51 +1097,10 @@ int batch_t(oidt_ctx *ctx, std::vector<Job *> &js, int nsteps) {
     if (j->pl.K != K) return fail(ctx, OIDT_ERR_INVALID, "batched jobs must share ring_steps");
     CU(ctx, cudaStreamWaitEvent(st, j->ready, 0));
   }
-  int left = nsteps;
-  while (left > 0) {
-    std::vector<uint64_t> ids;
-    std::vector<int> pars;
-    for (Job *j : js) ids.push_back(j->id), pars.push_back(j->parity);
-    // the cached composition of these jobs at these parities, else the least
-    // recently used slot
-    BatchPlan *hit = nullptr, *lru = &ctx->batch[0];
-    for (BatchPlan &c : ctx->batch) {
-      if (c.K == K && c.ids == ids && c.pars == pars) hit = &c;
-      if (c.last_use < lru->last_use) lru = &c;
-    }
-    if (!hit) {
-      drop_batch(*lru);
-      lru->ids = ids;
-      lru->pars = pars;
-      lru->K = K;
-      hit = lru;
-    }
-    BatchPlan &bp = *hit;
-    bp.last_use = ++ctx->batch_clock;
+  for (int left = nsteps; left > 0;) {
     const int cnt = std::min(K, left);
-    int rc = OIDT_OK;
-    if (cnt == K && (K & 1) == 0) {
-      if (!bp.graph) {
-        cudaGraph_t g;
-        const long long before = ctx->launches;
-        CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        rc = batch_block<T, EXACT>(ctx, js, K, st);
-        cudaError_t ce = cudaStreamEndCapture(st, &g);
-        if (rc) return rc;
-        CU(ctx, ce);
-        bp.graph_launches = ctx->launches - before;
-        ctx->launches = before;
-        CU(ctx, cudaGraphInstantiate(&bp.graph, g, 0));
-        CU(ctx, cudaGraphDestroy(g));
-      }
-      CU(ctx, cudaGraphLaunch(bp.graph, st));
-      ctx->launches += bp.graph_launches;
-    } else {
-      rc = batch_block<T, EXACT>(ctx, js, cnt, st);
-      if (rc) return rc;
-      if (cnt & 1)  // sweep jobs end this block on the other buffer
-        for (Job *j : js) j->parity ^= steps_flip(j);
-    }
+    int rc = batch_block<T, EXACT>(ctx, js, cnt, st);
+    if (rc) return rc;
     left -= cnt;
   }
   CU(ctx, cudaGetLastError());
@@ -1329,7 +1292,6 @@ int32_t oidt_destroy(oidt_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (auto &kv : ctx->jobs) destroy_job(ctx, kv.second);
     ctx->jobs.clear();
-    for (BatchPlan &bp : ctx->batch) drop_batch(bp);
     cudaStreamSynchronize(ctx->stream);
     for (int a = 0; a < kAuxStreams; ++a) {
       cudaStreamSynchronize(ctx->aux[a]);
@@ -1776,8 +1738,6 @@ int32_t oidt_job_release(oidt_ctx *ctx, uint64_t job) {
   if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
   CU(ctx, cudaSetDevice(ctx->device));
   CU(ctx, cudaEventSynchronize(J->done));
-  for (BatchPlan &bp : ctx->batch)
-    if (std::find(bp.ids.begin(), bp.ids.end(), job) != bp.ids.end()) drop_batch(bp);
   ctx->in_use -= J->pl.total;
   ctx->jobs.erase(job);
   destroy_job(ctx, J);

@@ -119,8 +119,8 @@ class Server:
         the requests whose last steps are now enqueued.  Whole ring blocks go
         through multi-job launches: block b advances every job with more than
         b blocks in its share, so the groups shrink as the small shares end
-        (each group's graph is cached by the engine); a share's last partial
-        block, if any, runs alone."""
+        (each job replays its own captured block graph, so changing groups
+        cost no capture); a share's last partial block, if any, runs alone."""
         jobs = []
         for (req, j, ji, adm) in self.active:
             jobs += [x for x in (j, ji) if x is not None and x.steps < x.spec.nt]
