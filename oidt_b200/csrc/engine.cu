@@ -7,18 +7,20 @@
 // reciprocals, CPML psi slabs in the reference's PSI_<F>_<A><LO|HI> shapes,
 // the source waveform, float64 twiddle tables [nf][nt], the capture ring
 // [K][port][slot][plane], float64 complex DFT accumulators
-// [port][comp][nf][plane], an optional line-probe record [4][nt][nx], and for
-// the 3D plane-sweep form a second field buffer and a second E-psi buffer (it
-// writes the other buffer each step).
+// [port][comp][nf][plane], the port-power result [nf], an optional line-probe
+// record [4][nt][nx], and for the 3D plane-sweep form a second field buffer and
+// a second E-psi buffer (it writes the other buffer each step).
 //
 // A time step is two per-cell launches (E half, H half; kernels.cuh) -- or,
 // for 3D jobs that ask for it, one plane-sweep launch over the job's work
 // items (sweep3d.cuh) -- then the line probe if the job has one.  Every K
 // steps a fold kernel turns the captured port planes into float64 DFT updates
 // and a one-thread kernel advances the step counter, so a K-step block is a
-// fixed launch sequence, captured once into a CUDA graph and replayed.  The
-// step kernels are launched with programmatic stream serialization and wait
-// for their predecessor in pdl_wait().
+// fixed launch sequence, captured once into a CUDA graph and replayed, alone
+// or as one branch of a multi-job block.  The step kernels are launched with
+// programmatic stream serialization and wait for their predecessor in
+// pdl_wait().  3D per-cell blocks are 32 x rows cells (rows 2, 4 or 8, a
+// launch choice that leaves results unchanged).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
