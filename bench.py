@@ -44,7 +44,7 @@ def dist_env():
 
 
 def dist_init(ws, local, backend="nccl"):
-    """Process group of the replica ranks (NCCL on the GPU box; gloo serves
+    """Process group of the replica ranks (NCCL on B200s; gloo serves
     the CPU tests of the same code).  A short timeout ends a rank that waits
     for a lost peer with an error instead of a hang."""
     if ws <= 1:

@@ -24,6 +24,6 @@ reproduce them bit for bit.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg may import, call, link or execute anything in this package, and only as
-the checker or the timed CPU baseline.  The product (``oidt_b200``) never
+the reference results the tests compare against or the timed CPU baseline.  The product (``oidt_b200``) never
 imports it and has no CPU fallback.
 """

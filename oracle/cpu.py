@@ -1,5 +1,5 @@
 """ctypes driver for the C oracle (``oracle/c/oracle.c``) -- TEST
-INFRASTRUCTURE ONLY (the timed CPU baseline and a fast float64 checker).
+INFRASTRUCTURE ONLY (the timed CPU baseline and fast float64 reference results for the tests).
 
 ``run_c(s, nsteps)`` advances an oracle state made by
 ``oracle.fdtd_ref.build`` / ``from_arrays`` in place, exactly as
