@@ -17,6 +17,7 @@ from .spec import DFT_COMPS, FIELD_ID, FIELDS, PSI, SimSpec, to_desc
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboidt.so")
 
+ABI_VERSION = 3  # OIDT_ABI_VERSION of include/oidt.h
 OK, ERR_INVALID, ERR_CUDA, ERR_BUDGET, ERR_NOTFOUND, ERR_TIMEOUT, ERR_STATE = 0, -1, -2, -3, -4, -5, -6
 EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error", "oidt_stats_get",
            "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
@@ -82,6 +83,10 @@ def load_library(path: str = LIB_PATH):
             "oidt_ctx_stream": ([vp, C.POINTER(vp)], i32),
             "oidt_job_profile": ([vp, u64, i32, C.POINTER(C.c_float)], i32),
         }
+        L.oidt_abi_version.argtypes, L.oidt_abi_version.restype = [], i32
+        if L.oidt_abi_version() != ABI_VERSION:
+            raise ImportError("%s has ABI %d, this package needs %d; rebuild it with `python -m oidt_b200.build`"
+                              % (path, L.oidt_abi_version(), ABI_VERSION))
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
             fn.argtypes = args

@@ -30,7 +30,9 @@ def test_library_exports_all_declared_symbols():
     assert set(EXPORTS) <= set(declared())
     f = lib.oidt_abi_version
     f.restype = ctypes.c_int32
-    assert f() == 3
+    from oidt_b200.engine import ABI_VERSION
+    header = open(os.path.join(ROOT, "include", "oidt.h")).read()
+    assert f() == ABI_VERSION == int(re.search(r"#define OIDT_ABI_VERSION (\d+)", header).group(1))
 
 
 def test_descriptor_validation_without_device():
@@ -75,3 +77,18 @@ def test_line_probe_descriptor_without_device():
     spec2.meta["probe"] = (5, 0)
     d2, keep2 = to_desc(spec2)
     assert lib.oidt_job_bytes(ctypes.byref(d2), ctypes.byref(b1)) == -1  # 2D: no line probe
+
+
+def test_library_of_another_abi_is_refused(tmp_path, monkeypatch):
+    """A stale liboidt.so (another OIDT_ABI_VERSION) is refused at load time
+    instead of being called with a descriptor it reads differently."""
+    import subprocess
+    from oidt_b200 import engine
+    src = tmp_path / "stub.c"
+    src.write_text("int oidt_abi_version(void) { return %d; }\n" % (engine.ABI_VERSION - 1))
+    so = tmp_path / "libstub.so"
+    subprocess.run(["gcc", "-shared", "-fPIC", "-o", str(so), str(src)], check=True)
+    monkeypatch.setattr(engine, "_lib", None)
+    with pytest.raises(ImportError, match="ABI %d" % (engine.ABI_VERSION - 1)):
+        engine.load_library(str(so))
+    assert engine._lib is None
