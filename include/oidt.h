@@ -31,8 +31,10 @@
 extern "C" {
 #endif
 
-#define OIDT_ABI_VERSION 3  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe);
-                              3: launch choices (reserved[2..3]), oidt_job_port_power */
+#define OIDT_ABI_VERSION 4  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe);
+                              3: launch choices (reserved[2..3]), oidt_job_port_power;
+                              4: oidt_job_read_dft_window_static, the vector launch form
+                                 (reserved[0] = 2) */
 
 /* status codes */
 #define OIDT_OK 0
@@ -100,7 +102,9 @@ typedef struct oidt_job_desc {
   const double *cos_e, *sin_e, *cos_h, *sin_h;
   int32_t ring_steps; /* steps buffered between DFT folds (0 = default)    */
   /* reserved[0]: 3D launch form, 0 = per-cell E-half / H-half launches,
-   *              1 = plane sweep (one launch per step);
+   *              1 = plane sweep (one launch per step),
+   *              2 = vector form: the E-half / H-half launches with four
+   *                  cells per thread along z and 16-byte accesses;
    * reserved[1]: 1 = launch every step directly (no CUDA-graph replay);
    * reserved[2]: 3D per-cell form only: rows of a block's 32 x rows tile,
    *              2, 4 or 8 (0 = 4);

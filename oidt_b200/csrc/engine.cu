@@ -41,6 +41,7 @@
 #include "../../include/oidt.h"
 #include "kernels.cuh"
 #include "sweep3d.cuh"
+#include "vec3d.cuh"
 
 using namespace oidt;
 
@@ -52,7 +53,7 @@ constexpr int kBlock3Z = 32, kRowsDefault = 4;  // 3D per-cell tile: 32 (k) x ro
 constexpr int kBlock2 = 128;
 constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
 constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread box
-constexpr int kVariantCell = 0, kVariantSweep = 1;  // oidt_job_desc.reserved[0]
+constexpr int kVariantCell = 0, kVariantSweep = 1, kVariantVec = 2;  // oidt_job_desc.reserved[0]
 
 // ---------------------------------------------------------------------------
 // Line probe (wave-impedance recording): after every step, colocated Ey, Ez,
@@ -110,83 +111,9 @@ template <typename T, bool EXACT, int BY>
 __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 4 ? 64 : 32) / BY) k_y3_e(Params<T> p, int s) {
   pdl_wait();
   const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * BY, i = blockIdx.z;
-  const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
+  const int k = k0 + threadIdx.x, j = j0 + threadIdx.y;
   if (!block_meets_src<BY>(p, i, j0, k0)) {
-    // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
-    // read below stays inside the grid arrays
-    if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
-    using A = Ar<T, EXACT>;
-    const int sy = p.nzp, nz = p.nz;
-    const long long sx = (long long)p.ny * p.nzp, bi = i * sx;
-    const int o = j * sy + k;  // offset inside the plane
-    const T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
-    const T hx0 = __ldg(hx + o), hy0 = __ldg(hy + o), hz0 = __ldg(hz + o);
-    const T dhz_y = A::sub(__ldg(hz + (o + sy)), hz0), dhy_z = A::sub(__ldg(hy + (o + 1)), hy0);
-    const T dhx_z = A::sub(__ldg(hx + (o + 1)), hx0), dhz_x = A::sub(__ldg(hz + sx + o), hz0);
-    const T dhy_x = A::sub(__ldg(hy + sx + o), hy0), dhx_y = A::sub(__ldg(hx + (o + sy)), hx0);
-    const T rkx = p.rkd[0][i], rky = p.rkd[1][j], rkz = p.rkd[2][k];
-    const T kx = EXACT ? p.kd[0][i] : T(0), ky = EXACT ? p.kd[1][j] : T(0), kz = EXACT ? p.kd[2][k] : T(0);
-    const T cb0 = __ldg(p.cb[0] + bi + o), cb1 = __ldg(p.cb[1] + bi + o), cb2 = __ldg(p.cb[2] + bi + o);
-    T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
-    T e[3];
-    e[0] = A::add(ex[o], A::mul(cb0, A::sub(A::div(dhz_y, ky, rky), A::div(dhy_z, kz, rkz))));
-    e[1] = A::add(ey[o], A::mul(cb1, A::sub(A::div(dhx_z, kz, rkz), A::div(dhz_x, kx, rkx))));
-    e[2] = A::add(ez[o], A::mul(cb2, A::sub(A::div(dhy_x, kx, rkx), A::div(dhx_y, ky, rky))));
-    // updated components: Ex i (ib,ie) j [jb,je) k [kb,ke); Ey i [ib,ie) j (jb,je) k [kb,ke);
-    // Ez i [ib,ie) j [jb,je) k (kb,ke)
-    const bool kc = k >= p.kb && k < p.ke, ko = k > p.kb && k < p.ke;
-    const bool mex = i > p.ib && kc, mey = j > p.jb && kc, mez = ko;
-    int d, side, q;
-    if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc, update_pml_ez_xinc
-      const int oa = (d * p.ny + j) * nz + k;
-      if (mey) {
-        T *const py = p.psi[EY][AX][side] + oa;
-        const T vy = A::add(A::mul(p.be[q], *py), A::div(A::mul(p.ce[q], dhz_x), p.dx, p.rdx));
-        *py = vy;
-        e[1] = A::sub(e[1], A::mul(cb1, vy));
-      }
-      if (mez) {
-        T *const pz = p.psi[EZ][AX][side] + oa;
-        const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhy_x), p.dx, p.rdx));
-        *pz = vz;
-        e[2] = A::add(e[2], A::mul(cb2, vz));
-      }
-    }
-    if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc, update_pml_ez_yinc
-      const int oa = (i * P + d) * nz + k;
-      if (mex) {
-        T *const px = p.psi[EX][AY][side] + oa;
-        const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhz_y), p.dx, p.rdx));
-        *px = vx;
-        e[0] = A::add(e[0], A::mul(cb0, vx));
-      }
-      if (mez) {
-        T *const pz = p.psi[EZ][AY][side] + oa;
-        const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhx_y), p.dx, p.rdx));
-        *pz = vz;
-        e[2] = A::sub(e[2], A::mul(cb2, vz));
-      }
-    }
-    if (kc && (q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ex_zinc, update_pml_ey_zinc
-      const int oa = (i * p.ny + j) * P + d;
-      if (mex) {
-        T *const px = p.psi[EX][AZ][side] + oa;
-        const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhy_z), p.dx, p.rdx));
-        *px = vx;
-        e[0] = A::sub(e[0], A::mul(cb0, vx));
-      }
-      if (mey) {
-        T *const py = p.psi[EY][AZ][side] + oa;
-        const T vy = A::add(A::mul(p.be[q], *py), A::div(A::mul(p.ce[q], dhx_z), p.dx, p.rdx));
-        *py = vy;
-        e[1] = A::add(e[1], A::mul(cb1, vy));
-      }
-    }
-    if (mex) ex[o] = e[0];
-    if (mey) ey[o] = e[1];
-    if (mez) ez[o] = e[2];
-    if (k == p.port_pos[0] || k == p.port_pos[1])
-      y3_capture_e(p, s, i, j, k, (mex ? 1 : 0) | (mey ? 2 : 0) | (mez ? 4 : 0), e);
+    y3_e_masked<T, EXACT>(p, i, j, k, s);
     return;
   }
   if (k >= p.nz || j >= p.ny) return;
@@ -198,84 +125,9 @@ __global__ void __launch_bounds__(32 * BY, (sizeof(T) == 4 ? 64 : 32) / BY) k_y3
   // planes in decreasing i: the H half starts on the E planes the E half wrote
   // last (still in L2), and ends on the planes the next E half reads first
   const int k0 = blockIdx.x * kBlock3Z, j0 = blockIdx.y * BY, i = gridDim.z - 1 - blockIdx.z;
-  const int k = k0 + threadIdx.x, j = j0 + threadIdx.y, P = p.P;
+  const int k = k0 + threadIdx.x, j = j0 + threadIdx.y;
   if (!block_meets_src<BY>(p, i, j0, k0)) {
-    // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
-    // read below stays inside the grid arrays (ib, jb >= 1)
-    if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
-    using A = Ar<T, EXACT>;
-    const int sy = p.nzp, nz = p.nz;
-    const long long sx = (long long)p.ny * p.nzp, bi = i * sx;
-    const int o = j * sy + k;  // offset inside the plane
-    const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
-    // updated components: Hx i [ib,ie) j (jb,je) k (kb,ke); Hy i (ib,ie) j [jb,je) k (kb,ke);
-    // Hz i (ib,ie) j (jb,je) k [kb,ke)
-    const bool ko = k > p.kb && k < p.ke, kc = k >= p.kb && k < p.ke;
-    const bool mhx = j > p.jb && ko, mhy = i > p.ib && ko, mhz = i > p.ib && j > p.jb && kc;
-    const T ex0 = __ldg(ex + o), ey0 = __ldg(ey + o), ez0 = __ldg(ez + o);
-    // (k - 1 is read only where k > kb >= 1)
-    const T dey_z = A::sub(ey0, ko ? __ldg(ey + (o - 1)) : ey0), dez_y = A::sub(ez0, __ldg(ez + (o - sy)));
-    const T dez_x = A::sub(ez0, __ldg(ez - sx + o)), dex_z = A::sub(ex0, ko ? __ldg(ex + (o - 1)) : ex0);
-    const T dex_y = A::sub(ex0, __ldg(ex + (o - sy))), dey_x = A::sub(ey0, __ldg(ey - sx + o));
-    const T rkx = p.rkd[3][i], rky = p.rkd[4][j], rkz = p.rkd[5][k];
-    const T kx = EXACT ? p.kd[3][i] : T(0), ky = EXACT ? p.kd[4][j] : T(0), kz = EXACT ? p.kd[5][k] : T(0);
-    const T db = p.db;
-    T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
-    T h[3];
-    h[0] = A::add(hx[o], A::mul(db, A::sub(A::div(dey_z, kz, rkz), A::div(dez_y, ky, rky))));
-    h[1] = A::add(hy[o], A::mul(db, A::sub(A::div(dez_x, kx, rkx), A::div(dex_z, kz, rkz))));
-    h[2] = A::add(hz[o], A::mul(db, A::sub(A::div(dex_y, ky, rky), A::div(dey_x, kx, rkx))));
-    int d, side, q;
-    if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hy_xinc, update_pml_hz_xinc
-      const int oa = (d * p.ny + j) * nz + k;
-      if (mhy) {
-        T *const py = p.psi[HY][AX][side] + oa;
-        const T vy = A::add(A::mul(p.bh[q], *py), A::div(A::mul(p.ch[q], dez_x), p.dx, p.rdx));
-        *py = vy;
-        h[1] = A::add(h[1], A::mul(db, vy));
-      }
-      if (mhz) {
-        T *const pz = p.psi[HZ][AX][side] + oa;
-        const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dey_x), p.dx, p.rdx));
-        *pz = vz;
-        h[2] = A::sub(h[2], A::mul(db, vz));
-      }
-    }
-    if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc, update_pml_hz_yinc
-      const int oa = (i * P + d) * nz + k;
-      if (mhx) {
-        T *const px = p.psi[HX][AY][side] + oa;
-        const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dez_y), p.dx, p.rdx));
-        *px = vx;
-        h[0] = A::sub(h[0], A::mul(db, vx));
-      }
-      if (mhz) {
-        T *const pz = p.psi[HZ][AY][side] + oa;
-        const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dex_y), p.dx, p.rdx));
-        *pz = vz;
-        h[2] = A::add(h[2], A::mul(db, vz));
-      }
-    }
-    if (ko && (q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hx_zinc, update_pml_hy_zinc
-      const int oa = (i * p.ny + j) * P + d;
-      if (mhx) {
-        T *const px = p.psi[HX][AZ][side] + oa;
-        const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dey_z), p.dx, p.rdx));
-        *px = vx;
-        h[0] = A::add(h[0], A::mul(db, vx));
-      }
-      if (mhy) {
-        T *const py = p.psi[HY][AZ][side] + oa;
-        const T vy = A::add(A::mul(p.bh[q], *py), A::div(A::mul(p.ch[q], dex_z), p.dx, p.rdx));
-        *py = vy;
-        h[1] = A::sub(h[1], A::mul(db, vy));
-      }
-    }
-    if (mhx) hx[o] = h[0];
-    if (mhy) hy[o] = h[1];
-    if (mhz) hz[o] = h[2];
-    if (k == p.port_pos[0] || k == p.port_pos[1] || k == p.port_pos[0] + 1 || k == p.port_pos[1] + 1)
-      y3_capture_h(p, s, i, j, k, (mhx ? 1 : 0) | (mhy ? 2 : 0) | (mhz ? 4 : 0), h);
+    y3_h_masked<T, EXACT>(p, i, j, k, s);
     return;
   }
   if (k >= p.nz || j >= p.ny) return;
@@ -456,10 +308,14 @@ std::vector<int> cb_of(int mode) {  // which cb slots are used
   return {0, 1, 2};
 }
 
-long long psi_elems(int mode, int axis, int nx, int ny, int nz, int P) {
+// Elements of one psi slab array in the reference's shape; `pitch` is the
+// device row length along z of the x- and y-slab arrays (nz, or nzp for the
+// vector form's 16-byte rows).
+long long psi_elems(int mode, int axis, int nx, int ny, int nz, int P, int pitch = 0) {
   if (mode != OIDT_MODE_YEE3D) return (long long)(axis == AX ? P * (long long)ny : (long long)nx * P);
-  if (axis == AX) return (long long)P * ny * nz;
-  if (axis == AY) return (long long)nx * P * nz;
+  const long long row = pitch > 0 ? pitch : nz;
+  if (axis == AX) return (long long)P * ny * row;
+  if (axis == AY) return (long long)nx * P * row;
   return (long long)nx * ny * P;
 }
 
@@ -473,6 +329,7 @@ struct JobPlan {
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
   int rows;  // 3D per-cell tile rows
+  int psi_pitch;  // row length along z of the 3D x- and y-slab psi arrays (nz or nzp)
 };
 
 // Flags of the work item whose E box starts at (y0 - 1, z0 - 1) (rows
@@ -595,9 +452,10 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   } else if (d->probe[1] != 0 || d->probe[2] != 0) {
     return bad("probe[1..2] must be 0 without a probe");
   }
-  if (d->reserved[0] != kVariantCell && d->reserved[0] != kVariantSweep) return bad("reserved[0]: launch form 0 or 1");
+  if (d->reserved[0] != kVariantCell && d->reserved[0] != kVariantSweep && d->reserved[0] != kVariantVec)
+    return bad("reserved[0]: launch form 0, 1 or 2");
   if (d->reserved[1] != 0 && d->reserved[1] != 1) return bad("reserved[1]: 0 or 1");
-  const int variant = is3 && d->reserved[0] == kVariantSweep ? kVariantSweep : kVariantCell;
+  const int variant = is3 ? d->reserved[0] : kVariantCell;
   const int rows = d->reserved[2] == 0 ? kRowsDefault : d->reserved[2];
   if (rows != 2 && rows != 4 && rows != 8) return bad("reserved[2]: tile rows 0 (default), 2, 4 or 8");
   if (d->reserved[2] != 0 && !(is3 && variant == kVariantCell))
@@ -612,6 +470,13 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   if (K > 4096) return bad("ring_steps too large");
   if (variant == kVariantSweep && (K & 1)) ++K;  // graphs of the sweep end on the parity they start
   const int nbuf = variant == kVariantSweep ? 2 : 1;
+  const int psi_pitch = variant == kVariantVec ? nzp : d->nz;
+  if (variant == kVariantVec) {  // 32-bit row offsets of the pitched slabs; x-planes on grid.y
+    const long long lim = 0x7fffffffLL;
+    if ((long long)P * d->ny * nzp > lim || (long long)d->nx * P * nzp > lim)
+      return bad("grid too large: a pitched CPML slab holds 2^31 or more elements");
+    if (d->ie - d->ib > 65535) return bad("vector form: at most 65535 updated x-planes");
+  }
   Layout L;
   memset(pl, 0, sizeof(*pl));
   for (int b = 0; b < nbuf; ++b)
@@ -620,8 +485,9 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   const int dims[3] = {d->nx, d->ny, d->nz};
   for (int a = 0; a < 6; ++a) {
     if (!is3 && (a == 2 || a == 5)) continue;
-    pl->off_kd[a] = L.take((size_t)dims[a % 3] * esz);
-    pl->off_rkd[a] = L.take((size_t)dims[a % 3] * esz);
+    // padded to whole 4-element groups (the vector form loads z kappa rows by 16 bytes)
+    pl->off_kd[a] = L.take(align_up(dims[a % 3], 4) * esz);
+    pl->off_rkd[a] = L.take(align_up(dims[a % 3], 4) * esz);
   }
   pl->off_be = L.take(P * esz);
   pl->off_ce = L.take(P * esz);
@@ -630,7 +496,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   for (auto fa : psi_pairs(d->mode))
     for (int b = 0; b < (is_e(fa.first) ? nbuf : 1); ++b)
       for (int sd = 0; sd < 2; ++sd)
-        pl->off_psi[b][fa.first][fa.second][sd] = L.take(psi_elems(d->mode, fa.second, d->nx, d->ny, d->nz, P) * esz);
+        pl->off_psi[b][fa.first][fa.second][sd] = L.take(psi_elems(d->mode, fa.second, d->nx, d->ny, d->nz, P, psi_pitch) * esz);
   pl->off_jsrc = L.take((size_t)d->nt * esz);
   for (int t = 0; t < 4; ++t) pl->off_tw[t] = L.take((size_t)d->nf * d->nt * 8);
   pl->off_ring = L.take((size_t)K * 2 * nslot_of(d->mode) * plane * esz);
@@ -653,6 +519,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->plane = plane;
   pl->K = K;
   pl->rows = rows;
+  pl->psi_pitch = psi_pitch;
   pl->esz = esz;
   pl->nzp = nzp;
   pl->nbuf = nbuf;
@@ -785,6 +652,7 @@ template <typename T> void fill_params(Job *J) {
     p.db = (T)d.db;
     p.dx = (T)d.dx;
     p.rdx = (T)(1.0 / (double)p.dx);
+    p.psx = p.psy = pl.psi_pitch;
     for (auto fa : psi_pairs(d.mode))
       for (int sd = 0; sd < 2; ++sd) {
         const bool two = is_e(fa.first) && pl.nbuf == 2;
@@ -934,6 +802,32 @@ void y3_half(int rows, bool H, bool pdl, const Params<T> &p, int s, cudaStream_t
   else y3_half_by<T, EXACT, 4>(H, pdl, p, s, st);
 }
 
+// Split of a 3D row between the vector form's roles: four-cell groups over
+// k in [kb + P, ke - P) rounded inward to multiples of 4, the rest one cell per
+// thread.
+template <typename T> VecGeom vec_geom(const Params<T> &p) {
+  VecGeom g;
+  g.kz0 = (p.kb + p.P + 3) / 4 * 4;
+  g.kz1 = (p.ke - p.P) / 4 * 4;
+  if (g.kz1 <= g.kz0) g.kz0 = g.kz1 = p.nzp;  // no z-clean group: every cell in the edge role
+  g.nvc = (g.kz1 - g.kz0) / 4;
+  g.nedge = g.kz0 + (p.nzp - g.kz1);
+  const long long rows = p.je - p.jb;
+  g.nb_vec = (int)((rows * g.nvc + kVecThreads - 1) / kVecThreads);
+  return g;
+}
+
+// One 3D vector-form half-step: the vector-role blocks, then the edge-role
+// blocks, of one x-plane per grid row.
+template <typename T, bool EXACT> void v3_half(bool H, bool pdl, const Params<T> &p, int s, cudaStream_t st) {
+  const VecGeom g = vec_geom(p);
+  const long long nb_edge = ((long long)(p.je - p.jb) * g.nedge + kVecThreads - 1) / kVecThreads;
+  const dim3 grd((unsigned)(g.nb_vec + nb_edge), p.ie - p.ib), blk(kVecThreads);
+  void (*kern)(Params<T>, VecGeom, int) = H ? k_v3_h<T, EXACT> : k_v3_e<T, EXACT>;
+  if (pdl) launch_step_kernel(kern, grd, blk, 0, st, p, g, s);
+  else kern<<<grd, blk, 0, st>>>(p, g, s);
+}
+
 template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, EYB, EZB, ST>(); }
 
 template <typename T, bool EXACT>
@@ -974,7 +868,10 @@ template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s,
     return;
   }
   Params<T> &p = cells<T>(J)[par];
-  if (J->d.mode == OIDT_MODE_YEE3D) {
+  if (J->pl.variant == kVariantVec) {
+    v3_half<T, EXACT>(false, true, p, s, st);
+    v3_half<T, EXACT>(true, true, p, s, st);
+  } else if (J->d.mode == OIDT_MODE_YEE3D) {
     y3_half<T, EXACT>(J->pl.rows, false, true, p, s, st);
     y3_half<T, EXACT>(J->pl.rows, true, true, p, s, st);
   } else {
@@ -1155,11 +1052,14 @@ template <typename T, bool EXACT> int profile_t(oidt_ctx *ctx, Job *J, int nstep
     }
     Params<T> &p = cells<T>(J)[par];
     if (J->d.mode == OIDT_MODE_YEE3D) {
+      const bool vec = J->pl.variant == kVariantVec;
       cudaEventRecord(ev[q++], st);
-      y3_half<T, EXACT>(J->pl.rows, false, false, p, s, st);
+      if (vec) v3_half<T, EXACT>(false, false, p, s, st);
+      else y3_half<T, EXACT>(J->pl.rows, false, false, p, s, st);
       cudaEventRecord(ev[q++], st);
       cudaEventRecord(ev[q++], st);
-      y3_half<T, EXACT>(J->pl.rows, true, false, p, s, st);
+      if (vec) v3_half<T, EXACT>(true, false, p, s, st);
+      else y3_half<T, EXACT>(J->pl.rows, true, false, p, s, st);
       cudaEventRecord(ev[q++], st);
       if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par, st);  // untimed
     } else {
@@ -1729,7 +1629,14 @@ int32_t oidt_job_read_psi(oidt_ctx *ctx, uint64_t job, int32_t field, int32_t ax
   int rc = read_common(ctx, J);
   if (rc) return rc;
   const int b = (is_e(field) && J->pl.nbuf == 2) ? J->parity : 0;
-  CU(ctx, cudaMemcpy(out, J->mem + J->pl.off_psi[b][field][axis][side], need, cudaMemcpyDeviceToHost));
+  const unsigned char *src = J->mem + J->pl.off_psi[b][field][axis][side];
+  const bool pitched = J->d.mode == OIDT_MODE_YEE3D && axis != AZ && J->pl.psi_pitch != J->d.nz;
+  if (pitched) {  // rows of nz cells out of rows of psi_pitch cells
+    const size_t row = (size_t)J->d.nz * J->pl.esz, pitch = (size_t)J->pl.psi_pitch * J->pl.esz;
+    CU(ctx, cudaMemcpy2D(out, row, src, pitch, row, need / row, cudaMemcpyDeviceToHost));
+  } else {
+    CU(ctx, cudaMemcpy(out, src, need, cudaMemcpyDeviceToHost));
+  }
   return OIDT_OK;
 }
 
@@ -1761,7 +1668,8 @@ int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
     for (int b = 0; b < (is_e(fa.first) ? pl.nbuf : 1); ++b)
       for (int sd = 0; sd < 2; ++sd)
         CU(ctx, cudaMemsetAsync(J->mem + pl.off_psi[b][fa.first][fa.second][sd], 0,
-                                psi_elems(J->d.mode, fa.second, J->d.nx, J->d.ny, J->d.nz, J->d.num_cpml) * pl.esz, st));
+                                psi_elems(J->d.mode, fa.second, J->d.nx, J->d.ny, J->d.nz, J->d.num_cpml,
+                                          pl.psi_pitch) * pl.esz, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_ring, 0, pl.off_acc - pl.off_ring, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_acc, 0, pl.off_state - pl.off_acc, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_state, 0, 64, st));

@@ -78,6 +78,8 @@ template <typename T> struct Params {
   T db, dx, rdx;
   T *psi[6][3][2];       // [field][slab axis][side] (read; H psi updated in place)
   T *psin[6][3][2];      // E psi written (== psi for the per-cell launches)
+  int psx, psy;          // row pitch (elements along z) of the x- and y-slab psi arrays:
+                         // nz (the reference layout) or nzp (16-byte rows, vector form)
   const void *tmap_f;    // plane sweep: 6 CUtensorMaps of f[] (device memory)
   const void *tmap_cb;   // plane sweep: 3 CUtensorMaps of cb[]
   int src_field;         // -1: none
@@ -96,12 +98,13 @@ __device__ __forceinline__ bool in_src(const Params<T> &p, int fld, int i, int j
          k >= p.slo[2] && k < p.shi[2];
 }
 
-// psi array index for a 3D slab array whose `axis` extent is P.
-__device__ __forceinline__ long long psi_idx3(int axis, int i, int j, int k, int nx, int ny, int nz,
-                                              int P) {
-  if (axis == AX) return ((long long)i * ny + j) * nz + k;  // i is the slab index d
-  if (axis == AY) return ((long long)i * P + j) * nz + k;   // j is d
-  return ((long long)i * ny + j) * P + k;                   // k is d
+// psi array index for a 3D slab array whose `axis` extent is P: x-slabs
+// [P][ny][psx], y-slabs [nx][P][psy], z-slabs [nx][ny][P].
+template <typename T>
+__device__ __forceinline__ long long psi_idx3(const Params<T> &p, int axis, int i, int j, int k) {
+  if (axis == AX) return ((long long)i * p.ny + j) * p.psx + k;  // i is the slab index d
+  if (axis == AY) return ((long long)i * p.P + j) * p.psy + k;   // j is d
+  return ((long long)i * p.ny + j) * p.P + k;                    // k is d
 }
 
 // E-field CPML slab test along one axis: returns coefficient index or -1,
@@ -156,7 +159,7 @@ template <typename T, bool EXACT, class Acc>
 __device__ __forceinline__ int y3_e_compute(const Params<T> &p, const Acc &a, int i, int j, int k, int n, bool own,
                                             T out[3]) {
   using A = Ar<T, EXACT>;
-  const int nx = p.nx, ny = p.ny, nz = p.nz, P = p.P;
+  const int P = p.P;
   const T Jn = p.src_field >= 0 ? p.jsrc[n] : T(0);
   int d, side, q, mask = 0;
   out[0] = a.eold(EX);
@@ -171,7 +174,7 @@ __device__ __forceinline__ int y3_e_compute(const Params<T> &p, const Acc &a, in
     T e = A::add(out[0], A::mul(cb, A::sub(A::div(dhz, p.kd[1][j], p.rkd[1][j]),
                                             A::div(dhy, p.kd[2][k], p.rkd[2][k]))));
     if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc :113-123
-      const long long o = psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      const long long o = psi_idx3(p, AY, i, d, k);
       T v = A::add(A::mul(p.be[q], p.psi[EX][AY][side][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
       if (own) p.psin[EX][AY][side][o] = v;
       e = A::add(e, A::mul(cb, v));
@@ -182,7 +185,7 @@ __device__ __forceinline__ int y3_e_compute(const Params<T> &p, const Acc &a, in
         if (in_src(p, HY, i, j, k + 1)) h1 = A::sub(h1, Jn);
         if (in_src(p, HY, i, j, k)) h0 = A::sub(h0, Jn);
       }
-      const long long o = psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      const long long o = psi_idx3(p, AZ, i, j, d);
       T v = A::add(A::mul(p.be[q], p.psi[EX][AZ][side][o]), A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
       if (own) p.psin[EX][AZ][side][o] = v;
       e = A::sub(e, A::mul(cb, v));
@@ -199,13 +202,13 @@ __device__ __forceinline__ int y3_e_compute(const Params<T> &p, const Acc &a, in
                                             A::div(dhz, p.kd[0][i], p.rkd[0][i]))));
     if (in_src(p, EY, i, j, k)) e = A::sub(e, Jn);       // update_source :104-110
     if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc :139-149
-      const long long o = psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      const long long o = psi_idx3(p, AX, d, j, k);
       T v = A::add(A::mul(p.be[q], p.psi[EY][AX][side][o]), A::div(A::mul(p.ce[q], dhz), p.dx, p.rdx));
       if (own) p.psin[EY][AX][side][o] = v;
       e = A::sub(e, A::mul(cb, v));
     }
     if ((q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ey_zinc :152-162
-      const long long o = psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      const long long o = psi_idx3(p, AZ, i, j, d);
       T v = A::add(A::mul(p.be[q], p.psi[EY][AZ][side][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
       if (own) p.psin[EY][AZ][side][o] = v;
       e = A::add(e, A::mul(cb, v));
@@ -227,13 +230,13 @@ __device__ __forceinline__ int y3_e_compute(const Params<T> &p, const Acc &a, in
         if (in_src(p, HY, i + 1, j, k)) h1 = A::sub(h1, Jn);
         if (in_src(p, HY, i, j, k)) h0 = A::sub(h0, Jn);
       }
-      const long long o = psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      const long long o = psi_idx3(p, AX, d, j, k);
       T v = A::add(A::mul(p.be[q], p.psi[EZ][AX][side][o]), A::div(A::mul(p.ce[q], A::sub(h1, h0)), p.dx, p.rdx));
       if (own) p.psin[EZ][AX][side][o] = v;
       e = A::add(e, A::mul(cb, v));
     }
     if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ez_yinc :178-188
-      const long long o = psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      const long long o = psi_idx3(p, AY, i, d, k);
       T v = A::add(A::mul(p.be[q], p.psi[EZ][AY][side][o]), A::div(A::mul(p.ce[q], dhx), p.dx, p.rdx));
       if (own) p.psin[EZ][AY][side][o] = v;
       e = A::sub(e, A::mul(cb, v));
@@ -249,7 +252,7 @@ __device__ __forceinline__ int y3_e_compute(const Params<T> &p, const Acc &a, in
 template <typename T, bool EXACT, class Acc>
 __device__ __forceinline__ int y3_h_compute(const Params<T> &p, const Acc &a, int i, int j, int k, int n, T out[3]) {
   using A = Ar<T, EXACT>;
-  const int nx = p.nx, ny = p.ny, nz = p.nz, P = p.P;
+  const int P = p.P;
   const T db = p.db;
   int d, side, q, mask = 0;
   out[0] = a.hold(HX);
@@ -262,13 +265,13 @@ __device__ __forceinline__ int y3_h_compute(const Params<T> &p, const Acc &a, in
     T h = A::add(out[0], A::mul(db, A::sub(A::div(dey, p.kd[5][k], p.rkd[5][k]),
                                             A::div(dez, p.kd[4][j], p.rkd[4][j]))));
     if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc :191-201
-      T *ps = p.psi[HX][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T *ps = p.psi[HX][AY][side] + psi_idx3(p, AY, i, d, k);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
       *ps = v;
       h = A::sub(h, A::mul(db, v));
     }
     if ((q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hx_zinc :204-214
-      T *ps = p.psi[HX][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T *ps = p.psi[HX][AZ][side] + psi_idx3(p, AZ, i, j, d);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
       *ps = v;
       h = A::add(h, A::mul(db, v));
@@ -285,13 +288,13 @@ __device__ __forceinline__ int y3_h_compute(const Params<T> &p, const Acc &a, in
     h = A::add(h, A::mul(db, A::sub(A::div(dez, p.kd[3][i], p.rkd[3][i]),
                                      A::div(dex, p.kd[5][k], p.rkd[5][k]))));
     if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hy_xinc :217-227
-      T *ps = p.psi[HY][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T *ps = p.psi[HY][AX][side] + psi_idx3(p, AX, d, j, k);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dez), p.dx, p.rdx));
       *ps = v;
       h = A::add(h, A::mul(db, v));
     }
     if ((q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hy_zinc :230-240
-      T *ps = p.psi[HY][AZ][side] + psi_idx3(AZ, i, j, d, nx, ny, nz, P);
+      T *ps = p.psi[HY][AZ][side] + psi_idx3(p, AZ, i, j, d);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
       *ps = v;
       h = A::sub(h, A::mul(db, v));
@@ -306,13 +309,13 @@ __device__ __forceinline__ int y3_h_compute(const Params<T> &p, const Acc &a, in
     T h = A::add(out[2], A::mul(db, A::sub(A::div(dex, p.kd[4][j], p.rkd[4][j]),
                                             A::div(dey, p.kd[3][i], p.rkd[3][i]))));
     if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hz_xinc :243-253
-      T *ps = p.psi[HZ][AX][side] + psi_idx3(AX, d, j, k, nx, ny, nz, P);
+      T *ps = p.psi[HZ][AX][side] + psi_idx3(p, AX, d, j, k);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dey), p.dx, p.rdx));
       *ps = v;
       h = A::sub(h, A::mul(db, v));
     }
     if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hz_yinc :256-266
-      T *ps = p.psi[HZ][AY][side] + psi_idx3(AY, i, d, k, nx, ny, nz, P);
+      T *ps = p.psi[HZ][AY][side] + psi_idx3(p, AY, i, d, k);
       T v = A::add(A::mul(p.bh[q], *ps), A::div(A::mul(p.ch[q], dex), p.dx, p.rdx));
       *ps = v;
       h = A::add(h, A::mul(db, v));
@@ -374,6 +377,177 @@ __device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int 
   if (m & 2) p.f[HY][c] = h[1];
   if (m & 4) p.f[HZ][c] = h[2];
   y3_capture_h(p, s, i, j, k, m, h);
+}
+
+// E update of one cell (i, j, k) of a block away from the source box: the
+// three curl updates, then the CPML terms -- x and y slabs uniform over a
+// warp of 32 consecutive k, z slab per lane -- each component stored where its
+// (i, j, k) range holds (operation order as y3_e_compute, which it equals cell
+// by cell).  Nothing is updated outside [ib, ie) x [jb, je); inside, every
+// neighbour read stays inside the grid arrays.  Grid arrays are addressed as
+// a per-plane base plus a 32-bit offset inside the plane (plan_job rejects
+// grids whose plane or slab sizes would not fit).
+template <typename T, bool EXACT>
+__device__ __forceinline__ void y3_e_masked(const Params<T> &p, int i, int j, int k, int s) {
+  const int P = p.P;
+  // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
+  // read below stays inside the grid arrays
+  if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
+  using A = Ar<T, EXACT>;
+  const int sy = p.nzp, nz = p.nz;
+  const long long sx = (long long)p.ny * p.nzp, bi = i * sx;
+  const int o = j * sy + k;  // offset inside the plane
+  const T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
+  const T hx0 = __ldg(hx + o), hy0 = __ldg(hy + o), hz0 = __ldg(hz + o);
+  const T dhz_y = A::sub(__ldg(hz + (o + sy)), hz0), dhy_z = A::sub(__ldg(hy + (o + 1)), hy0);
+  const T dhx_z = A::sub(__ldg(hx + (o + 1)), hx0), dhz_x = A::sub(__ldg(hz + sx + o), hz0);
+  const T dhy_x = A::sub(__ldg(hy + sx + o), hy0), dhx_y = A::sub(__ldg(hx + (o + sy)), hx0);
+  const T rkx = p.rkd[0][i], rky = p.rkd[1][j], rkz = p.rkd[2][k];
+  const T kx = EXACT ? p.kd[0][i] : T(0), ky = EXACT ? p.kd[1][j] : T(0), kz = EXACT ? p.kd[2][k] : T(0);
+  const T cb0 = __ldg(p.cb[0] + bi + o), cb1 = __ldg(p.cb[1] + bi + o), cb2 = __ldg(p.cb[2] + bi + o);
+  T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
+  T e[3];
+  e[0] = A::add(ex[o], A::mul(cb0, A::sub(A::div(dhz_y, ky, rky), A::div(dhy_z, kz, rkz))));
+  e[1] = A::add(ey[o], A::mul(cb1, A::sub(A::div(dhx_z, kz, rkz), A::div(dhz_x, kx, rkx))));
+  e[2] = A::add(ez[o], A::mul(cb2, A::sub(A::div(dhy_x, kx, rkx), A::div(dhx_y, ky, rky))));
+  // updated components: Ex i (ib,ie) j [jb,je) k [kb,ke); Ey i [ib,ie) j (jb,je) k [kb,ke);
+  // Ez i [ib,ie) j [jb,je) k (kb,ke)
+  const bool kc = k >= p.kb && k < p.ke, ko = k > p.kb && k < p.ke;
+  const bool mex = i > p.ib && kc, mey = j > p.jb && kc, mez = ko;
+  int d, side, q;
+  if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc, update_pml_ez_xinc
+    const int oa = (d * p.ny + j) * p.psx + k;
+    if (mey) {
+      T *const py = p.psi[EY][AX][side] + oa;
+      const T vy = A::add(A::mul(p.be[q], *py), A::div(A::mul(p.ce[q], dhz_x), p.dx, p.rdx));
+      *py = vy;
+      e[1] = A::sub(e[1], A::mul(cb1, vy));
+    }
+    if (mez) {
+      T *const pz = p.psi[EZ][AX][side] + oa;
+      const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhy_x), p.dx, p.rdx));
+      *pz = vz;
+      e[2] = A::add(e[2], A::mul(cb2, vz));
+    }
+  }
+  if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc, update_pml_ez_yinc
+    const int oa = (i * P + d) * p.psy + k;
+    if (mex) {
+      T *const px = p.psi[EX][AY][side] + oa;
+      const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhz_y), p.dx, p.rdx));
+      *px = vx;
+      e[0] = A::add(e[0], A::mul(cb0, vx));
+    }
+    if (mez) {
+      T *const pz = p.psi[EZ][AY][side] + oa;
+      const T vz = A::add(A::mul(p.be[q], *pz), A::div(A::mul(p.ce[q], dhx_y), p.dx, p.rdx));
+      *pz = vz;
+      e[2] = A::sub(e[2], A::mul(cb2, vz));
+    }
+  }
+  if (kc && (q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ex_zinc, update_pml_ey_zinc
+    const int oa = (i * p.ny + j) * P + d;
+    if (mex) {
+      T *const px = p.psi[EX][AZ][side] + oa;
+      const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhy_z), p.dx, p.rdx));
+      *px = vx;
+      e[0] = A::sub(e[0], A::mul(cb0, vx));
+    }
+    if (mey) {
+      T *const py = p.psi[EY][AZ][side] + oa;
+      const T vy = A::add(A::mul(p.be[q], *py), A::div(A::mul(p.ce[q], dhx_z), p.dx, p.rdx));
+      *py = vy;
+      e[1] = A::add(e[1], A::mul(cb1, vy));
+    }
+  }
+  if (mex) ex[o] = e[0];
+  if (mey) ey[o] = e[1];
+  if (mez) ez[o] = e[2];
+  if (k == p.port_pos[0] || k == p.port_pos[1])
+    y3_capture_e(p, s, i, j, k, (mex ? 1 : 0) | (mey ? 2 : 0) | (mez ? 4 : 0), e);
+}
+
+// H update of one cell (i, j, k) away from the source box (as y3_h_compute;
+// ib, jb >= 1, so every neighbour read stays inside the grid arrays).
+template <typename T, bool EXACT>
+__device__ __forceinline__ void y3_h_masked(const Params<T> &p, int i, int j, int k, int s) {
+  const int P = p.P;
+  // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
+  // read below stays inside the grid arrays (ib, jb >= 1)
+  if (i < p.ib || i >= p.ie || j < p.jb || j >= p.je || k >= p.nz) return;
+  using A = Ar<T, EXACT>;
+  const int sy = p.nzp, nz = p.nz;
+  const long long sx = (long long)p.ny * p.nzp, bi = i * sx;
+  const int o = j * sy + k;  // offset inside the plane
+  const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
+  // updated components: Hx i [ib,ie) j (jb,je) k (kb,ke); Hy i (ib,ie) j [jb,je) k (kb,ke);
+  // Hz i (ib,ie) j (jb,je) k [kb,ke)
+  const bool ko = k > p.kb && k < p.ke, kc = k >= p.kb && k < p.ke;
+  const bool mhx = j > p.jb && ko, mhy = i > p.ib && ko, mhz = i > p.ib && j > p.jb && kc;
+  const T ex0 = __ldg(ex + o), ey0 = __ldg(ey + o), ez0 = __ldg(ez + o);
+  // (k - 1 is read only where k > kb >= 1)
+  const T dey_z = A::sub(ey0, ko ? __ldg(ey + (o - 1)) : ey0), dez_y = A::sub(ez0, __ldg(ez + (o - sy)));
+  const T dez_x = A::sub(ez0, __ldg(ez - sx + o)), dex_z = A::sub(ex0, ko ? __ldg(ex + (o - 1)) : ex0);
+  const T dex_y = A::sub(ex0, __ldg(ex + (o - sy))), dey_x = A::sub(ey0, __ldg(ey - sx + o));
+  const T rkx = p.rkd[3][i], rky = p.rkd[4][j], rkz = p.rkd[5][k];
+  const T kx = EXACT ? p.kd[3][i] : T(0), ky = EXACT ? p.kd[4][j] : T(0), kz = EXACT ? p.kd[5][k] : T(0);
+  const T db = p.db;
+  T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
+  T h[3];
+  h[0] = A::add(hx[o], A::mul(db, A::sub(A::div(dey_z, kz, rkz), A::div(dez_y, ky, rky))));
+  h[1] = A::add(hy[o], A::mul(db, A::sub(A::div(dez_x, kx, rkx), A::div(dex_z, kz, rkz))));
+  h[2] = A::add(hz[o], A::mul(db, A::sub(A::div(dex_y, ky, rky), A::div(dey_x, kx, rkx))));
+  int d, side, q;
+  if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hy_xinc, update_pml_hz_xinc
+    const int oa = (d * p.ny + j) * p.psx + k;
+    if (mhy) {
+      T *const py = p.psi[HY][AX][side] + oa;
+      const T vy = A::add(A::mul(p.bh[q], *py), A::div(A::mul(p.ch[q], dez_x), p.dx, p.rdx));
+      *py = vy;
+      h[1] = A::add(h[1], A::mul(db, vy));
+    }
+    if (mhz) {
+      T *const pz = p.psi[HZ][AX][side] + oa;
+      const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dey_x), p.dx, p.rdx));
+      *pz = vz;
+      h[2] = A::sub(h[2], A::mul(db, vz));
+    }
+  }
+  if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc, update_pml_hz_yinc
+    const int oa = (i * P + d) * p.psy + k;
+    if (mhx) {
+      T *const px = p.psi[HX][AY][side] + oa;
+      const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dez_y), p.dx, p.rdx));
+      *px = vx;
+      h[0] = A::sub(h[0], A::mul(db, vx));
+    }
+    if (mhz) {
+      T *const pz = p.psi[HZ][AY][side] + oa;
+      const T vz = A::add(A::mul(p.bh[q], *pz), A::div(A::mul(p.ch[q], dex_y), p.dx, p.rdx));
+      *pz = vz;
+      h[2] = A::add(h[2], A::mul(db, vz));
+    }
+  }
+  if (ko && (q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hx_zinc, update_pml_hy_zinc
+    const int oa = (i * p.ny + j) * P + d;
+    if (mhx) {
+      T *const px = p.psi[HX][AZ][side] + oa;
+      const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dey_z), p.dx, p.rdx));
+      *px = vx;
+      h[0] = A::add(h[0], A::mul(db, vx));
+    }
+    if (mhy) {
+      T *const py = p.psi[HY][AZ][side] + oa;
+      const T vy = A::add(A::mul(p.bh[q], *py), A::div(A::mul(p.ch[q], dex_z), p.dx, p.rdx));
+      *py = vy;
+      h[1] = A::sub(h[1], A::mul(db, vy));
+    }
+  }
+  if (mhx) hx[o] = h[0];
+  if (mhy) hy[o] = h[1];
+  if (mhz) hz[o] = h[2];
+  if (k == p.port_pos[0] || k == p.port_pos[1] || k == p.port_pos[0] + 1 || k == p.port_pos[1] + 1)
+    y3_capture_h(p, s, i, j, k, (mhx ? 1 : 0) | (mhy ? 2 : 0) | (mhz ? 4 : 0), h);
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,377 @@
+// vec3d.cuh -- 3D Yee E and H half-steps, vector form.
+//
+// One launch per half-step, in two roles over one x-plane per grid row:
+//
+// * vector role: the z-clean cells, k in [kz0, kz1) = [kb + P, ke - P)
+//   rounded inward to multiples of 4, where no cell is in a z slab or on the
+//   rim.  A thread owns four consecutive cells along z (the guide axis,
+//   contiguous in memory) of one (i, j) row.  Rows are padded to nzp (a
+//   multiple of 4 cells) and every sub-buffer starts on a 256-byte boundary,
+//   so each field, dt/eps grid, z kappa array and x/y-slab psi row moves in
+//   16-byte accesses (float4, or two double2 in float64).  The x-slab terms
+//   are uniform over a block and the y-slab terms over a row, and so are the
+//   component update ranges (only i = ib and j = jb leave a component out):
+//   no per-cell test runs in this role.  A plane is a flat list of (row,
+//   four-cell group) pairs, so no lane idles whatever nz is.
+// * edge role: every other cell (the z slabs and the rim, 9 % of the cells
+//   of a 256-cell guide with a 10-cell CPML), one per thread, through the
+//   per-cell code of kernels.cuh (y3_e_masked / y3_h_masked).
+//
+// Per cell the arithmetic is the sequence of kernels.cuh's y3_e_compute /
+// y3_h_compute (the reference's fdtd_funcs.py:43-266 in its launch order):
+// curl update, soft source, then the CPML terms of the x, y and z slabs.  With
+// EXACT arithmetic every operation is the reference's IEEE operation, so
+// float64 runs equal the reference and the oracle bit for bit.
+//
+// Cells next to the source box take the general per-cell path (y3_e_cell /
+// y3_h_cell) in both roles of the E half-step: with the 'TM' source (Hy) the
+// reference subtracts J from Hy between the E curl and the E CPML kernels, so
+// the x-slab term of Ez and the z-slab term of Ex read Hy - J there.
+#pragma once
+#include "kernels.cuh"
+
+namespace oidt {
+
+constexpr int kVecThreads = 128;
+
+template <typename T> struct V4 { T v[4]; };
+
+// read-only data of this launch (non-coherent path)
+__device__ __forceinline__ void ld4(V4<float> &a, const float *p) {
+  const float4 x = __ldg(reinterpret_cast<const float4 *>(p));
+  a.v[0] = x.x; a.v[1] = x.y; a.v[2] = x.z; a.v[3] = x.w;
+}
+__device__ __forceinline__ void ld4(V4<double> &a, const double *p) {
+  const double2 x = __ldg(reinterpret_cast<const double2 *>(p)), y = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  a.v[0] = x.x; a.v[1] = x.y; a.v[2] = y.x; a.v[3] = y.y;
+}
+// data this launch also writes (each element only by the thread reading it)
+__device__ __forceinline__ void ldw4(V4<float> &a, const float *p) {
+  const float4 x = *reinterpret_cast<const float4 *>(p);
+  a.v[0] = x.x; a.v[1] = x.y; a.v[2] = x.z; a.v[3] = x.w;
+}
+__device__ __forceinline__ void ldw4(V4<double> &a, const double *p) {
+  const double2 x = reinterpret_cast<const double2 *>(p)[0], y = reinterpret_cast<const double2 *>(p)[1];
+  a.v[0] = x.x; a.v[1] = x.y; a.v[2] = y.x; a.v[3] = y.y;
+}
+__device__ __forceinline__ void st4(float *p, const float (&v)[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double *p, const double (&v)[4]) {
+  reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// Split of a row between the roles (computed on the host per job).
+struct VecGeom {
+  int kz0, kz1;  // vector role: k in [kz0, kz1), multiples of 4
+  int nvc;       // four-cell groups per row in the vector role
+  int nedge;     // edge-role cells per row: [0, kz0) and [kz1, nzp)
+  int nb_vec;    // blocks of the vector role per plane (the edge role follows)
+};
+
+// One cell within one cell of the source box (widened below in i and k: the
+// E CPML of Ex and Ez reads the Hy source at k + 1 and i + 1).
+template <typename T> __device__ __forceinline__ bool near_src(const Params<T> &p, int i, int j, int k0, int nk) {
+  return p.src_field >= 0 && i >= p.slo[0] - 1 && i < p.shi[0] && j >= p.slo[1] && j < p.shi[1] &&
+         k0 + nk > p.slo[2] - 1 && k0 < p.shi[2];
+}
+
+// Edge role: thread t of the plane's edge cells, one cell.
+template <typename T, bool EXACT, bool H>
+__device__ __forceinline__ void v3_edge(const Params<T> &p, const VecGeom &g, int i, int s) {
+  const int t = (blockIdx.x - g.nb_vec) * kVecThreads + threadIdx.x;
+  if (t >= (p.je - p.jb) * g.nedge) return;
+  const int r = t / g.nedge, e = t - r * g.nedge;
+  const int j = p.jb + r, k = e < g.kz0 ? e : g.kz1 + (e - g.kz0);
+  if (k >= p.nz) return;
+  if (near_src(p, i, j, k, 1)) {
+    if (H) y3_h_cell<T, EXACT>(p, i, j, k, p.state[0] + s, s);
+    else y3_e_cell<T, EXACT>(p, i, j, k, p.state[0] + s, s);
+  } else {
+    if (H) y3_h_masked<T, EXACT>(p, i, j, k, s);
+    else y3_e_masked<T, EXACT>(p, i, j, k, s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// E half-step.  Updated: Ex i (ib,ie) j [jb,je) k [kb,ke); Ey i [ib,ie)
+// j (jb,je) k [kb,ke); Ez i [ib,ie) j [jb,je) k (kb,ke).  Grid: (vector-role
+// then edge-role blocks, x-planes ib..ie-1).
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(kVecThreads) k_v3_e(Params<T> p, VecGeom g, int s) {
+  pdl_wait();
+  const int i = p.ib + blockIdx.y;
+  if ((int)blockIdx.x >= g.nb_vec) {
+    v3_edge<T, EXACT, false>(p, g, i, s);
+    return;
+  }
+  const int t = blockIdx.x * kVecThreads + threadIdx.x;
+  if (t >= (p.je - p.jb) * g.nvc) return;
+  const int r = t / g.nvc;
+  const int j = p.jb + r, k0 = g.kz0 + 4 * (t - r * g.nvc);
+  if (near_src(p, i, j, k0, 4) && p.src_field == HY) {
+    for (int m = 0; m < 4; ++m) y3_e_cell<T, EXACT>(p, i, j, k0 + m, p.state[0] + s, s);
+    return;
+  }
+  using A = Ar<T, EXACT>;
+  const int sy = p.nzp;
+  const long long sx = (long long)p.ny * p.nzp, bi = (long long)i * sx;
+  const int o = j * sy + k0;
+  const T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
+  V4<T> Hx, Hy, Hz, Hzy, Hxy, Hzx, Hyx, C0, C1, C2, Ex, Ey, Ez, Rz, Kz;
+  ld4(Hx, hx + o);
+  ld4(Hy, hy + o);
+  ld4(Hz, hz + o);
+  ld4(Hzy, hz + (o + sy));
+  ld4(Hxy, hx + (o + sy));
+  ld4(Hzx, hz + sx + o);
+  ld4(Hyx, hy + sx + o);
+  const T hyk = __ldg(hy + (o + 4)), hxk = __ldg(hx + (o + 4));  // k0 + 4 < kz1 <= nz - 2
+  ld4(C0, p.cb[0] + bi + o);
+  ld4(C1, p.cb[1] + bi + o);
+  ld4(C2, p.cb[2] + bi + o);
+  T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
+  ldw4(Ex, ex + o);
+  ldw4(Ey, ey + o);
+  ldw4(Ez, ez + o);
+  ld4(Rz, p.rkd[2] + k0);
+  if (EXACT) ld4(Kz, p.kd[2] + k0);
+  const T rkx = p.rkd[0][i], rky = p.rkd[1][j];
+  const T kx = EXACT ? p.kd[0][i] : T(0), ky = EXACT ? p.kd[1][j] : T(0);
+  // update ranges: all four cells are inside (kb, ke); Ex leaves out i = ib,
+  // Ey j = jb
+  const bool mex = i > p.ib, mey = j > p.jb;
+  T e0[4], e1[4], e2[4], dzy[4], dyz[4], dxz[4], dzx[4], dyx[4], dxy[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const T hy1 = m < 3 ? Hy.v[m + 1] : hyk, hx1 = m < 3 ? Hx.v[m + 1] : hxk;
+    const T kz = EXACT ? Kz.v[m] : T(0);
+    dzy[m] = A::sub(Hzy.v[m], Hz.v[m]);
+    dyz[m] = A::sub(hy1, Hy.v[m]);
+    dxz[m] = A::sub(hx1, Hx.v[m]);
+    dzx[m] = A::sub(Hzx.v[m], Hz.v[m]);
+    dyx[m] = A::sub(Hyx.v[m], Hy.v[m]);
+    dxy[m] = A::sub(Hxy.v[m], Hx.v[m]);
+    e0[m] = A::add(Ex.v[m], A::mul(C0.v[m], A::sub(A::div(dzy[m], ky, rky), A::div(dyz[m], kz, Rz.v[m]))));
+    e1[m] = A::add(Ey.v[m], A::mul(C1.v[m], A::sub(A::div(dxz[m], kz, Rz.v[m]), A::div(dzx[m], kx, rkx))));
+    e2[m] = A::add(Ez.v[m], A::mul(C2.v[m], A::sub(A::div(dyx[m], kx, rkx), A::div(dxy[m], ky, rky))));
+  }
+  // soft source on Ey ('TE'): after the curl, before the CPML terms
+  if (p.src_field == EY && mey && i >= p.slo[0] && i < p.shi[0] && j >= p.slo[1] && j < p.shi[1] &&
+      k0 + 4 > p.slo[2] && k0 < p.shi[2]) {
+    const T Jn = p.jsrc[p.state[0] + s];
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+      if (k0 + m >= p.slo[2] && k0 + m < p.shi[2]) e1[m] = A::sub(e1[m], Jn);
+  }
+  const int P = p.P;
+  int d, side, q;
+  if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc, update_pml_ez_xinc
+    const long long oa = ((long long)d * p.ny + j) * p.psx + k0;
+    const T be = p.be[q], ce = p.ce[q];
+    if (mey) {
+      T *const py = p.psi[EY][AX][side] + oa;
+      V4<T> Py;
+      ldw4(Py, py);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        Py.v[m] = A::add(A::mul(be, Py.v[m]), A::div(A::mul(ce, dzx[m]), p.dx, p.rdx));
+        e1[m] = A::sub(e1[m], A::mul(C1.v[m], Py.v[m]));
+      }
+      st4(py, Py.v);
+    }
+    T *const pz = p.psi[EZ][AX][side] + oa;
+    V4<T> Pz;
+    ldw4(Pz, pz);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      Pz.v[m] = A::add(A::mul(be, Pz.v[m]), A::div(A::mul(ce, dyx[m]), p.dx, p.rdx));
+      e2[m] = A::add(e2[m], A::mul(C2.v[m], Pz.v[m]));
+    }
+    st4(pz, Pz.v);
+  }
+  if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc, update_pml_ez_yinc
+    const long long oa = ((long long)i * P + d) * p.psy + k0;
+    const T be = p.be[q], ce = p.ce[q];
+    if (mex) {
+      T *const px = p.psi[EX][AY][side] + oa;
+      V4<T> Px;
+      ldw4(Px, px);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        Px.v[m] = A::add(A::mul(be, Px.v[m]), A::div(A::mul(ce, dzy[m]), p.dx, p.rdx));
+        e0[m] = A::add(e0[m], A::mul(C0.v[m], Px.v[m]));
+      }
+      st4(px, Px.v);
+    }
+    T *const pz = p.psi[EZ][AY][side] + oa;
+    V4<T> Pz;
+    ldw4(Pz, pz);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      Pz.v[m] = A::add(A::mul(be, Pz.v[m]), A::div(A::mul(ce, dxy[m]), p.dx, p.rdx));
+      e2[m] = A::sub(e2[m], A::mul(C2.v[m], Pz.v[m]));
+    }
+    st4(pz, Pz.v);
+  }
+  if (mex) st4(ex + o, e0);
+  if (mey) st4(ey + o, e1);
+  st4(ez + o, e2);
+  // port planes: raw Ex, Ey samples for the DFT fold
+#pragma unroll
+  for (int pq = 0; pq < 2; ++pq) {
+    const int dm = p.port_pos[pq] - k0;
+    if ((unsigned)dm < 4u) {
+      const long long pc = (long long)i * p.ny + j;
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+        if (m == dm) {
+          if (mex) capture(p, s, pq, 0, pc, e0[m]);
+          if (mey) capture(p, s, pq, 1, pc, e1[m]);
+        }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// H half-step.  Updated: Hx i [ib,ie) j (jb,je) k (kb,ke); Hy i (ib,ie)
+// j [jb,je) k (kb,ke); Hz i (ib,ie) j (jb,je) k [kb,ke).  Planes run in
+// decreasing i: the launch starts on the E planes the E half-step wrote last
+// (still in L2) and ends on the planes the next E half-step reads first.
+// ---------------------------------------------------------------------------
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(kVecThreads) k_v3_h(Params<T> p, VecGeom g, int s) {
+  pdl_wait();
+  const int i = p.ie - 1 - blockIdx.y;
+  if ((int)blockIdx.x >= g.nb_vec) {
+    v3_edge<T, EXACT, true>(p, g, i, s);
+    return;
+  }
+  const int t = blockIdx.x * kVecThreads + threadIdx.x;
+  if (t >= (p.je - p.jb) * g.nvc) return;
+  const int r = t / g.nvc;
+  const int j = p.jb + r, k0 = g.kz0 + 4 * (t - r * g.nvc);
+  using A = Ar<T, EXACT>;
+  const int sy = p.nzp;
+  const long long sx = (long long)p.ny * p.nzp, bi = (long long)i * sx;
+  const int o = j * sy + k0;
+  const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
+  V4<T> Ex, Ey, Ez, Ezy, Exy, Ezx, Eyx, Hx, Hy, Hz, Rz, Kz;
+  ld4(Ex, ex + o);
+  ld4(Ey, ey + o);
+  ld4(Ez, ez + o);
+  ld4(Ezy, ez + (o - sy));
+  ld4(Exy, ex + (o - sy));
+  ld4(Ezx, ez - sx + o);
+  ld4(Eyx, ey - sx + o);
+  const T eyk = __ldg(ey + (o - 1)), exk = __ldg(ex + (o - 1));  // k0 - 1 >= kz0 - 1 >= kb + P - 1
+  T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
+  ldw4(Hx, hx + o);
+  ldw4(Hy, hy + o);
+  ldw4(Hz, hz + o);
+  ld4(Rz, p.rkd[5] + k0);
+  if (EXACT) ld4(Kz, p.kd[5] + k0);
+  const T rkx = p.rkd[3][i], rky = p.rkd[4][j];
+  const T kx = EXACT ? p.kd[3][i] : T(0), ky = EXACT ? p.kd[4][j] : T(0);
+  const T db = p.db;
+  // update ranges: all four cells are inside (kb, ke); Hx leaves out j = jb,
+  // Hy i = ib, Hz both
+  const bool mhx = j > p.jb, mhy = i > p.ib, mhz = mhx && mhy;
+  // soft source on Hy ('TM'): subtracted before the Hy update
+  const bool src = p.src_field == HY && mhy && i >= p.slo[0] && i < p.shi[0] && j >= p.slo[1] && j < p.shi[1] &&
+                   k0 + 4 > p.slo[2] && k0 < p.shi[2];
+  const T Jn = src ? p.jsrc[p.state[0] + s] : T(0);
+  T h0[4], h1[4], h2[4], dyz[4], dzy[4], dzx[4], dxz[4], dxy[4], dyx[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const T ey1 = m > 0 ? Ey.v[m - 1] : eyk, ex1 = m > 0 ? Ex.v[m - 1] : exk;
+    const T kz = EXACT ? Kz.v[m] : T(0);
+    dyz[m] = A::sub(Ey.v[m], ey1);
+    dzy[m] = A::sub(Ez.v[m], Ezy.v[m]);
+    dzx[m] = A::sub(Ez.v[m], Ezx.v[m]);
+    dxz[m] = A::sub(Ex.v[m], ex1);
+    dxy[m] = A::sub(Ex.v[m], Exy.v[m]);
+    dyx[m] = A::sub(Ey.v[m], Eyx.v[m]);
+    T hy0 = Hy.v[m];
+    if (src && k0 + m >= p.slo[2] && k0 + m < p.shi[2]) hy0 = A::sub(hy0, Jn);
+    h0[m] = A::add(Hx.v[m], A::mul(db, A::sub(A::div(dyz[m], kz, Rz.v[m]), A::div(dzy[m], ky, rky))));
+    h1[m] = A::add(hy0, A::mul(db, A::sub(A::div(dzx[m], kx, rkx), A::div(dxz[m], kz, Rz.v[m]))));
+    h2[m] = A::add(Hz.v[m], A::mul(db, A::sub(A::div(dxy[m], ky, rky), A::div(dyx[m], kx, rkx))));
+  }
+  const int P = p.P;
+  int d, side, q;
+  if (mhy && (q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hy_xinc, update_pml_hz_xinc
+    const long long oa = ((long long)d * p.ny + j) * p.psx + k0;
+    const T bh = p.bh[q], ch = p.ch[q];
+    T *const py = p.psi[HY][AX][side] + oa;
+    V4<T> Py;
+    ldw4(Py, py);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      Py.v[m] = A::add(A::mul(bh, Py.v[m]), A::div(A::mul(ch, dzx[m]), p.dx, p.rdx));
+      h1[m] = A::add(h1[m], A::mul(db, Py.v[m]));
+    }
+    st4(py, Py.v);
+    if (mhz) {
+      T *const pz = p.psi[HZ][AX][side] + oa;
+      V4<T> Pz;
+      ldw4(Pz, pz);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        Pz.v[m] = A::add(A::mul(bh, Pz.v[m]), A::div(A::mul(ch, dyx[m]), p.dx, p.rdx));
+        h2[m] = A::sub(h2[m], A::mul(db, Pz.v[m]));
+      }
+      st4(pz, Pz.v);
+    }
+  }
+  if (mhx && (q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc, update_pml_hz_yinc
+    const long long oa = ((long long)i * P + d) * p.psy + k0;
+    const T bh = p.bh[q], ch = p.ch[q];
+    T *const px = p.psi[HX][AY][side] + oa;
+    V4<T> Px;
+    ldw4(Px, px);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      Px.v[m] = A::add(A::mul(bh, Px.v[m]), A::div(A::mul(ch, dzy[m]), p.dx, p.rdx));
+      h0[m] = A::sub(h0[m], A::mul(db, Px.v[m]));
+    }
+    st4(px, Px.v);
+    if (mhz) {
+      T *const pz = p.psi[HZ][AY][side] + oa;
+      V4<T> Pz;
+      ldw4(Pz, pz);
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        Pz.v[m] = A::add(A::mul(bh, Pz.v[m]), A::div(A::mul(ch, dxy[m]), p.dx, p.rdx));
+        h2[m] = A::add(h2[m], A::mul(db, Pz.v[m]));
+      }
+      st4(pz, Pz.v);
+    }
+  }
+  if (mhx) st4(hx + o, h0);
+  if (mhy) st4(hy + o, h1);
+  if (mhz) st4(hz + o, h2);
+  // port planes: raw Hx, Hy at k = port and port + 1
+#pragma unroll
+  for (int pq = 0; pq < 2; ++pq) {
+    const int dm = p.port_pos[pq] - k0;
+    if ((unsigned)(dm + 1) < 5u) {  // k = port or port + 1 among the four cells
+      const long long pc = (long long)i * p.ny + j;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        if (m == dm) {
+          if (mhx) capture(p, s, pq, 2, pc, h0[m]);
+          if (mhy) capture(p, s, pq, 4, pc, h1[m]);
+        }
+        if (m == dm + 1) {
+          if (mhx) capture(p, s, pq, 3, pc, h0[m]);
+          if (mhy) capture(p, s, pq, 5, pc, h1[m]);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace oidt

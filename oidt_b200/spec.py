@@ -84,7 +84,7 @@ class JobDesc(C.Structure):
     ]
 
 
-VARIANTS = {"cell": 0, "sweep": 1}
+VARIANTS = {"cell": 0, "sweep": 1, "vec": 2}
 
 
 def power_window(spec: SimSpec):
@@ -103,8 +103,9 @@ def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int 
     ``keepalive`` must outlive the ``oidt_job_create`` call.
 
     ``variant`` (3D only): 'cell' (default) -- the per-cell E-half / H-half
-    launches; 'sweep' -- one plane-sweep launch per step (E and H fused,
-    TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
+    launches; 'vec' -- the same two half-steps with four cells per thread
+    along z and 16-byte accesses; 'sweep' -- one plane-sweep launch per step
+    (E and H fused, TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
     launches every step directly instead of replaying K-step CUDA graphs.
     ``rows`` (3D per-cell form): tile rows of a block, 2, 4 or 8 (0 = 4);
     ``march_depth`` (3D plane sweep): x-planes per work item (0 = the

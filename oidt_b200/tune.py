@@ -3,8 +3,9 @@ results unchanged and keep the fastest.
 
 The choices are ``Engine.submit`` keywords:
 
-* ``variant`` -- 'cell', the per-cell E-half / H-half launches, or 'sweep',
-  one fused plane-sweep launch per step (TMA-staged tiles);
+* ``variant`` -- 'cell', the per-cell E-half / H-half launches; 'vec', the
+  same half-steps with four cells per thread along z and 16-byte accesses;
+  or 'sweep', one fused plane-sweep launch per step (TMA-staged tiles);
 * ``rows`` -- per-cell form: a block is a tile of 32 cells along z (the guide
   axis, contiguous) by ``rows`` rows along y, rows 2, 4 or 8;
 * ``march_depth`` -- plane sweep: x-planes per work item (0 = the engine's
@@ -36,6 +37,7 @@ from .spec import SimSpec
 
 DEFAULT = {"variant": "cell", "rows": 0, "march_depth": 0}
 CANDIDATES = (
+    {"variant": "vec", "rows": 0, "march_depth": 0},
     {"variant": "cell", "rows": 4, "march_depth": 0},
     {"variant": "cell", "rows": 2, "march_depth": 0},
     {"variant": "cell", "rows": 8, "march_depth": 0},
@@ -45,7 +47,9 @@ CANDIDATES = (
 
 
 def label(choice: dict) -> str:
-    """'cell/rows4', 'sweep/depth16', 'sweep/depth-auto'."""
+    """'vec', 'cell/rows4', 'sweep/depth16', 'sweep/depth-auto'."""
+    if choice["variant"] == "vec":
+        return "vec"
     if choice["variant"] == "cell":
         return "cell/rows%d" % (choice["rows"] or 4)
     return "sweep/depth%s" % (choice["march_depth"] or "-auto")

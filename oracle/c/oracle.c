@@ -1,5 +1,5 @@
 /*
- * oracle.c -- TEST INFRASTRUCTURE ONLY: a plain-C, float64, OpenMP
+ * oracle.c -- TEST INFRASTRUCTURE ONLY: a plain-C, float64 (or float32), OpenMP
  * restatement of the reference's S-parameter time loop, used as the timed CPU
  * baseline and cross-checked bit for bit against the NumPy oracle
  * (oracle/fdtd_ref.py).  Never linked into the product.
@@ -15,16 +15,24 @@
 #include <stddef.h>
 #include <stdint.h>
 
+/* Field, coefficient and psi type: double (the parity oracle) or, built with
+ * -DORACLE_REAL=float, float (the CPU timing at the reference's default
+ * float32 precision).  DFT accumulators and twiddles are double in both. */
+#ifndef ORACLE_REAL
+#define ORACLE_REAL double
+#endif
+typedef ORACLE_REAL real;
+
 typedef struct {
   int nx, ny, nz, P, ib, jb, kb, ie, je, ke;
-  double *f[6];          /* EX EY EZ HX HY HZ (reference layout) */
-  const double *cb[3];   /* CBX CBY CBZ */
-  const double *kd[6];   /* kxe kye kze kxh kyh kzh */
-  const double *be, *ce, *bh, *ch;
-  double db, dx;
-  double *psi[6][3][2];  /* [field][axis][lo/hi] */
+  real *f[6];            /* EX EY EZ HX HY HZ (reference layout) */
+  const real *cb[3];     /* CBX CBY CBZ */
+  const real *kd[6];     /* kxe kye kze kxh kyh kzh */
+  const real *be, *ce, *bh, *ch;
+  real db, dx;
+  real *psi[6][3][2];    /* [field][axis][lo/hi] */
   int src_field, slo[3], shi[3];
-  const double *jsrc;
+  const real *jsrc;
   int port[2];
   int nf, nt;
   const double *tw[4];   /* cosE sinE cosH sinH [nf][nt] */
@@ -37,8 +45,8 @@ enum { EX, EY, EZ, HX, HY, HZ };
 static void src3(OracleState *s, int n) {
   if (s->src_field < 0) return;
   const int ny = s->ny, nz = s->nz;
-  double *F = s->f[s->src_field];
-  const double J = s->jsrc[n];
+  real *F = s->f[s->src_field];
+  const real J = s->jsrc[n];
 #pragma omp parallel for collapse(2) schedule(static)
   for (int i = s->slo[0]; i < s->shi[0]; ++i)
     for (int j = s->slo[1]; j < s->shi[1]; ++j)
@@ -48,20 +56,20 @@ static void src3(OracleState *s, int n) {
 /* E-field CPML along `axis` for field E using the H difference along that
  * axis; t0/t1 give the transverse ranges (as [lo, hi) per axis, the slab axis
  * entry ignored).  sign +1: E + cb psi, -1: E - cb psi. */
-static void pml_e3(OracleState *s, int fe, int fh, int axis, int sign, const double *cb, const int lo[3],
+static void pml_e3(OracleState *s, int fe, int fh, int axis, int sign, const real *cb, const int lo[3],
                    const int hi[3]) {
   const int nx = s->nx, ny = s->ny, nz = s->nz, P = s->P;
   const int b = axis == 0 ? s->ib : axis == 1 ? s->jb : s->kb;
   const int e = axis == 0 ? s->ie : axis == 1 ? s->je : s->ke;
-  double *E = s->f[fe];
-  const double *H = s->f[fh];
+  real *E = s->f[fe];
+  const real *H = s->f[fh];
   int r0[3] = {lo[0], lo[1], lo[2]}, r1[3] = {hi[0], hi[1], hi[2]};
   r0[axis] = 0;
   r1[axis] = P;
   const long long st = axis == 0 ? (long long)ny * nz : axis == 1 ? nz : 1;
   const int pd[3] = {axis == 0 ? P : nx, axis == 1 ? P : ny, axis == 2 ? P : nz};
   for (int side = 0; side < 2; ++side) {
-    double *ps = s->psi[fe][axis][side];
+    real *ps = s->psi[fe][axis][side];
 #pragma omp parallel for collapse(2) schedule(static)
     for (int i = r0[0]; i < r1[0]; ++i)
       for (int j = r0[1]; j < r1[1]; ++j)
@@ -86,15 +94,15 @@ static void pml_h3(OracleState *s, int fh, int fe, int axis, int sign, const int
   const int nx = s->nx, ny = s->ny, nz = s->nz, P = s->P;
   const int b = axis == 0 ? s->ib : axis == 1 ? s->jb : s->kb;
   const int e = axis == 0 ? s->ie : axis == 1 ? s->je : s->ke;
-  double *H = s->f[fh];
-  const double *E = s->f[fe];
+  real *H = s->f[fh];
+  const real *E = s->f[fe];
   int r0[3] = {lo[0], lo[1], lo[2]}, r1[3] = {hi[0], hi[1], hi[2]};
   r0[axis] = 1;
   r1[axis] = P;
   const long long st = axis == 0 ? (long long)ny * nz : axis == 1 ? nz : 1;
   const int pd[3] = {axis == 0 ? P : nx, axis == 1 ? P : ny, axis == 2 ? P : nz};
   for (int side = 0; side < 2; ++side) {
-    double *ps = s->psi[fh][axis][side];
+    real *ps = s->psi[fh][axis][side];
 #pragma omp parallel for collapse(2) schedule(static)
     for (int i = r0[0]; i < r1[0]; ++i)
       for (int j = r0[1]; j < r1[1]; ++j)
@@ -117,8 +125,8 @@ static void pml_h3(OracleState *s, int fh, int fe, int axis, int sign, const int
 static void step3(OracleState *s, int n) {
   const int nx = s->nx, ny = s->ny, nz = s->nz;
   const int ib = s->ib, jb = s->jb, kb = s->kb, ie = s->ie, je = s->je, ke = s->ke;
-  double *Ex = s->f[EX], *Ey = s->f[EY], *Ez = s->f[EZ], *Hx = s->f[HX], *Hy = s->f[HY], *Hz = s->f[HZ];
-  const double *kxe = s->kd[0], *kye = s->kd[1], *kze = s->kd[2], *kxh = s->kd[3], *kyh = s->kd[4], *kzh = s->kd[5];
+  real *Ex = s->f[EX], *Ey = s->f[EY], *Ez = s->f[EZ], *Hx = s->f[HX], *Hy = s->f[HY], *Hz = s->f[HZ];
+  const real *kxe = s->kd[0], *kye = s->kd[1], *kze = s->kd[2], *kxh = s->kd[3], *kyh = s->kd[4], *kzh = s->kd[5];
   const long long SX = (long long)ny * nz, SY = nz;
   /* update_ex / update_ey / update_ez  (fdtd_funcs.py:43-70) */
 #pragma omp parallel for collapse(2) schedule(static)
@@ -160,7 +168,7 @@ static void step3(OracleState *s, int n) {
     pml_e3(s, EZ, HX, 1, -1, s->cb[2], lo, hi);
   }
   /* update_hx / update_hy / update_hz  (fdtd_funcs.py:73-100) */
-  const double db = s->db;
+  const real db = s->db;
 #pragma omp parallel for collapse(2) schedule(static)
   for (int i = ib; i < ie; ++i)
     for (int j = jb + 1; j < je; ++j)
@@ -235,9 +243,9 @@ static void step3(OracleState *s, int n) {
 /* 2D TM (Ez, Hx, Hy) -- FDTD_2D_TM/.../fdtd_funcs.py:43-144 */
 static void step_tm2(OracleState *s, int n) {
   const int nx = s->nx, ny = s->ny, P = s->P, ib = s->ib, jb = s->jb, ie = s->ie, je = s->je;
-  double *Ez = s->f[EZ], *Hx = s->f[HX], *Hy = s->f[HY];
-  const double *cb = s->cb[2], *kxe = s->kd[0], *kye = s->kd[1], *kxh = s->kd[3], *kyh = s->kd[4];
-  const double db = s->db, dx = s->dx;
+  real *Ez = s->f[EZ], *Hx = s->f[HX], *Hy = s->f[HY];
+  const real *cb = s->cb[2], *kxe = s->kd[0], *kye = s->kd[1], *kxh = s->kd[3], *kyh = s->kd[4];
+  const real db = s->db, dx = s->dx;
 #define I2(i, j) ((long long)(i) * ny + (j))
 #pragma omp parallel for schedule(static)
   for (int i = ib; i < ie; ++i)
@@ -249,7 +257,7 @@ static void step_tm2(OracleState *s, int n) {
     for (int i = s->slo[0]; i < s->shi[0]; ++i)
       for (int j = s->slo[1]; j < s->shi[1]; ++j) Ez[I2(i, j)] = Ez[I2(i, j)] - s->jsrc[n];
   {
-    double *lo = s->psi[EZ][0][0], *hi = s->psi[EZ][0][1];
+    real *lo = s->psi[EZ][0][0], *hi = s->psi[EZ][0][1];
     for (int i = 0; i < P; ++i)
       for (int j = jb; j < je; ++j) {
         long long c = I2(ib + i, j), p = (long long)i * ny + j;
@@ -284,7 +292,7 @@ static void step_tm2(OracleState *s, int n) {
       Hy[c] = Hy[c] + db * (Ez[c] - Ez[c - ny]) / kxh[i];
     }
   {
-    double *lo = s->psi[HX][1][0], *hi = s->psi[HX][1][1];
+    real *lo = s->psi[HX][1][0], *hi = s->psi[HX][1][1];
     for (int i = ib; i < ie; ++i)
       for (int j = 1; j < P; ++j) {
         long long c = I2(i, jb + j), p = (long long)i * P + j;
@@ -340,3 +348,4 @@ int oracle_run(OracleState *s, int mode, int n0, int count) {
 }
 
 int oracle_state_size(void) { return (int)sizeof(OracleState); }
+int oracle_real_size(void) { return (int)sizeof(real); }

@@ -52,7 +52,7 @@ MUT3 = [
     ("win_lo[1]", -1), ("win_hi[1]", 19), ("win_hi[0]", 20), ("win_lo[0]", 16),
     ("src_field", 6), ("src_lo[2]", 1), ("src_hi[1]", 19),
     ("probe[0]", 2), ("probe[1]", 3),
-    ("reserved[0]", 2), ("reserved[1]", 2), ("reserved[2]", 3), ("reserved[3]", 4),
+    ("reserved[0]", 3), ("reserved[1]", 2), ("reserved[2]", 3), ("reserved[3]", 4),
     ("ring_steps", 4097),
 ]
 

@@ -44,11 +44,17 @@ def test_descriptor_launch_choices_validated_on_host():
         assert _bytes(lib, d)[0] == 0, depth
     d, keep = to_desc(spec, variant="sweep", march_depth=-1)
     assert _bytes(lib, d)[0] == -1
+    d, keep = to_desc(spec, variant="vec")  # the vector form: x/y-slab psi rows padded like the fields
+    rc, vec = _bytes(lib, d)
+    assert rc == 0 and vec >= base
+    for bad in (dict(rows=2), dict(march_depth=4)):  # neither choice belongs to the vector form
+        d, keep = to_desc(spec, variant="vec", **bad)
+        assert _bytes(lib, d)[0] == -1, bad
     slab = W.slab2d(nx=60, ny=50, P=5, core_cells=6, src_x=10, ports=(15, 45), steps=10, nf=3)
     d, keep = to_desc(slab, rows=2)  # 2D has one launch form
     assert _bytes(lib, d)[0] == -1
     d, keep = to_desc(slab)
-    d.reserved[0] = 2  # no such launch form
+    d.reserved[0] = 3  # no such launch form
     assert _bytes(lib, d)[0] == -1
 
 
@@ -65,7 +71,7 @@ class _FakeTuner(tune.Tuner):
         return self.fake[tune.label(choice)]
 
 
-TIMES = {"cell/rows4": 0.090, "cell/rows2": 0.093, "cell/rows8": 0.088, "sweep/depth-auto": 0.140,
+TIMES = {"vec": 0.089, "cell/rows4": 0.090, "cell/rows2": 0.093, "cell/rows8": 0.088, "sweep/depth-auto": 0.140,
          "sweep/depth16": 0.150}
 
 
