@@ -11,6 +11,24 @@ FDTD/GPU/FDTD_3D/s-parameter_extraction/fdtd_main.py:431, in G).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
+``roofline`` is the time step against the HBM bound: the compulsory bytes of
+one step (every field read and written once, the three dt/eps grids read once
+-- 60 B per cell in FP32 -- plus 8 B per CPML psi element, 8 P (ny nz + nx nz
++ nx ny) of them) over the graph-replayed step time, against the measured copy
+bandwidth.
+
+At N = 1 the line also carries the other workloads, each with its own clock
+record: ``serving`` (Poisson arrivals of mixed 2D/3D roughness jobs at 20/s
+for 60 s under a 150 GB HBM budget, with |S - S_FP64| of a seeded sample),
+``batched`` (64 uneven roughness realizations, batched against one at a time),
+``slab2d`` (the 2D TMz slab) and ``large`` (a 151 M-cell rib guide, FP32
+against FP64 on the GPU).
+
+``--impl reference`` times the CPU restatement of the same loop (C/OpenMP, the
+oracle) on the host cores: each bench step is a fixed sample of consecutive
+time steps of the same simulation, in float32 (the engine's precision), with a
+float64 sample beside it.
+
 Multi-GPU (torchrun, one rank per GPU): every rank runs its own independent
 simulation (replicas; the path has no exchange step), the timed region is
 bracketed by barriers and the slowest rank's time is used.
@@ -130,23 +148,19 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # helpers
 # ---------------------------------------------------------------------------
-def psi_elements(spec):
-    from oidt_b200.spec import PSI
-    return sum(2 * int(np.prod(spec.psi_shape(axis))) for _, axis in PSI[spec.mode])
-
-
 def psi_elements_of(spec, half):
     """CPML psi elements updated by the E or H half-step (both sides)."""
     from oidt_b200.spec import PSI
     return sum(2 * int(np.prod(spec.psi_shape(axis))) for f, axis in PSI[spec.mode] if f.startswith(half))
 
 
-def algorithmic_bytes(spec, esz=4):
-    """Compulsory HBM bytes of the two per-cell launches of one 3D time step.
-    E half-step: H (3 words), E (3) and dt/eps (3) read, E (3) written = 12
-    words per cell; H half-step: E (3) and H (3) read, H (3) written = 9 words
-    per cell; each CPML psi element read and written once.  DFT capture,
-    source and twiddle traffic are not credited."""
+def half_step_bytes(spec, esz=4):
+    """Bytes each half-step launch moves at least: E half-step H (3 words), E
+    (3) and dt/eps (3) read, E (3) written = 12 words per cell; H half-step E
+    (3) and H (3) read, H (3) written = 9 words per cell; each CPML psi
+    element read and written once.  Per-launch diagnostics only: the two
+    launches re-read each other's fields, which the step's compulsory bytes do
+    not count."""
     return {"E": 12 * esz * spec.ncells + 2 * esz * psi_elements_of(spec, "E"),
             "H": 9 * esz * spec.ncells + 2 * esz * psi_elements_of(spec, "H")}
 
@@ -159,19 +173,32 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-PROFILE = os.path.join(ROOT, "profiles", "k_y3_e_strip3d_128x128x256.txt")
+PROFILE = os.path.join(ROOT, "profiles", "v3_step_strip3d_128x128x256.txt")
 
 
 def ncu_traffic():
-    """DRAM bytes of one E half-step launch (dram__bytes_read.sum +
-    dram__bytes_write.sum) from the committed ncu summary (key=value line
-    ``dram_bytes_per_launch=``)."""
+    """DRAM bytes of one time step (dram__bytes_read.sum +
+    dram__bytes_write.sum of the E and H half-step launches and the step's
+    share of the DFT fold) from the committed ncu summary (key=value line
+    ``dram_bytes_per_step=``)."""
     if not os.path.exists(PROFILE):
         return None
     for line in open(PROFILE):
-        if line.startswith("dram_bytes_per_launch="):
+        if line.startswith("dram_bytes_per_step="):
             return float(line.split("=", 1)[1])
     return None
+
+
+SAMPLE_STEPS = 150  # time steps per CPU sample (reference-arm step, CPU baseline)
+
+
+def bench_config(spec, ws):
+    """The workload description both arms print."""
+    from oidt_b200.spec import PSI
+    state_mb = (spec.ncells * 9 + sum(2 * int(np.prod(spec.psi_shape(a))) for _, a in PSI[spec.mode])) * 4 / 1e6
+    return {"workload": WORKLOAD_NAME, "grid": list(spec.shape), "steps_per_sim": spec.nt, "nf": spec.nf,
+            "parallelism": "replicas x%d" % ws,
+            "l2": "inputs larger than L2 (%.0f MB device state per run > 126 MB)" % state_mb}
 
 
 def pinned_spec(spec, prec):
@@ -230,36 +257,69 @@ def measure_slab2d(eng):
     return out
 
 
-def cpu_baseline(spec, target_s=15.0):
-    """Float64 oracle on the same workload, a bounded number of time steps."""
+def cpu_baseline(spec, samples=3):
+    """The C/OpenMP oracle on the host cores, float32 (the engine's precision)
+    and float64: ``samples`` timed samples of SAMPLE_STEPS consecutive time
+    steps of the same workload each, after one untimed sample."""
     from oracle import cpu as OC
-    return OC.time_steps(spec, target_s=target_s)
+    f32, _ = OC.time_steps(spec, nsteps=SAMPLE_STEPS, samples=samples, precision="float32")
+    f64, _ = OC.time_steps(spec, nsteps=SAMPLE_STEPS, samples=samples, precision="float64")
+    return dict(f32, float64=f64)
 
 
 # ---------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------
 def run_reference(args, ws, rank, local):
+    """The reference arm: the CPU restatement of the path on the host cores,
+    rank 0 only.  One bench step is one sample of SAMPLE_STEPS consecutive
+    time steps, continuing one simulation (a fresh one, untimed, when the
+    workload's steps run out); value = cells x time steps / CPU time in
+    float32, with a float64 sample of the same length beside it."""
     if rank != 0:
         return 0
     from oidt_b200 import workloads as W
+    from oracle import cpu as OC
+    from oracle import fdtd_ref as R
     spec = W.strip3d(**WORKLOAD)
-    vals = []
-    info = None
-    for _ in range(args.warmup):
-        cpu_baseline(spec, target_s=min(5.0, args.cpu_seconds))
-    for _ in range(args.steps):
-        info = cpu_baseline(spec, target_s=args.cpu_seconds)
-        vals.append(info["value"])
-    v = float(np.median(vals))
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": info["ms_per_time_step"] * spec.nt, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "grid": list(spec.shape), "steps_per_sim": spec.nt, "nf": spec.nf},
-            "cpu_baseline": dict(info, value=v),
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    s = R.from_spec(spec)
+    ms = []
+    for it in range(args.warmup + args.steps):
+        if s.n + SAMPLE_STEPS > spec.nt:
+            s = R.from_spec(spec)
+        t0 = time.perf_counter()
+        OC.run_c(s, SAMPLE_STEPS, "float32")
+        dt = (time.perf_counter() - t0) * 1e3
+        if it >= args.warmup:
+            ms.append(dt)
+    ms_step = float(np.mean(ms))
+    v = spec.ncells * SAMPLE_STEPS / (ms_step * 1e-3) / 1e9
+    f64, _ = OC.time_steps(spec, nsteps=SAMPLE_STEPS, samples=3, precision="float64")
+    sample = "%d consecutive time steps of the %d-step simulation per bench step, float32 fields (float64 DFT), " \
+             "C/OpenMP restatement of the path" % (SAMPLE_STEPS, spec.nt)
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 3),
+            "step": "%d time steps" % SAMPLE_STEPS, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": bench_config(spec, ws),
+            "cpu_baseline": {"value": round(v, 5), "unit": UNIT, "cores": OC.threads(), "kind": "port",
+                             "precision": "float32", "sample": sample, "ms_per_time_step": round(ms_step / SAMPLE_STEPS, 4),
+                             "float64": f64},
+            "e2e": {"value": round(v, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def with_clocks(device, fn, *a, **kw):
+    """fn's result with the clock record sampled while it ran."""
+    clk = ClockSampler(device)
+    clk.start()
+    try:
+        out = fn(*a, **kw)
+    finally:
+        rec = clk.stop()
+    if isinstance(out, dict):
+        out["clocks"] = rec
+    return out
 
 
 def run_engine(args, ws, rank, local):
@@ -267,6 +327,7 @@ def run_engine(args, ws, rank, local):
     from oidt_b200.build import build
     from oidt_b200 import workloads as W
     from oidt_b200.engine import Engine
+    from oidt_b200.large import roofline_bytes
     build()
     dist = dist_init(ws, local)
     torch.cuda.set_device(local)
@@ -299,10 +360,14 @@ def run_engine(args, ws, rank, local):
     ms = dist_max(dist, ms, local)
     value = whole_job_rate(ws, spec.ncells, spec.nt, ms)
 
-    # ---- per-kernel roofline (live CUDA events on the engine stream) -----
-    # A time step is two launches, the E half-step (k_y3_e, the larger one)
-    # and the H half-step (k_y3_h); profile() times each launch with CUDA
-    # events on the engine's stream, without graph replay.
+    # ---- roofline of the time step ----------------------------------------
+    # achieved = compulsory bytes of one step / graph-replayed step time; the
+    # per-launch figures (CUDA events on the engine stream around each
+    # launch, no graph replay) explain it.
+    peak, peak_kind = measured_peaks()
+    step_bytes = roofline_bytes(spec)
+    ms_ts = ms / spec.nt
+    achieved = step_bytes / (ms_ts * 1e-3) / 1e9
     job.reset()
     job.advance(200)  # fields populated, source on
     prof = [job.profile(16) for _ in range(4)]
@@ -310,11 +375,7 @@ def run_engine(args, ws, rank, local):
     ms_h = float(np.median([p[1] for p in prof]))
     ms_fold = float(np.median([p[2] for p in prof]))
     job.sync()
-    alg = algorithmic_bytes(spec)
-    achieved = alg["E"] / (ms_e * 1e-3) / 1e9
-    achieved_h = alg["H"] / (ms_h * 1e-3) / 1e9
-    peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic()
+    half = half_step_bytes(spec)
     job.release()
 
     # ---- end to end through the C ABI, host buffers ---------------------
@@ -342,50 +403,91 @@ def run_engine(args, ws, rank, local):
     e2e = dist_max(dist, float(np.mean(e2e_ms)), local)
     e2e_value = whole_job_rate(ws, spec.ncells, spec.nt, e2e)
 
-    # ---- batched realizations and the served mix (one GPU: at N > 1 they
-    # would hold every GPU while rank 0 alone works) -------------------------
-    batched = serving = slab2d = None
+    # ---- the other workloads (one GPU: at N > 1 they would hold every GPU
+    # while rank 0 alone works) -----------------------------------------------
+    extra = {}
     if rank == 0 and ws == 1 and not args.no_extra:
-        from oidt_b200 import batch as B, serve as SV
+        from oidt_b200 import batch as B, large as L, serve as SV
         # serving first: its latencies then see no host state left by the
-        # batched leg's 64 realization specs
-        serving = SV.measure(eng, rate_hz=20.0, duration_s=args.serve_window)
-        batched = B.measure(eng, n=args.batch_n, steps=3000)
-        slab2d = measure_slab2d(eng)
+        # batched leg's 64 realization specs; its context has the 150 GB budget
+        eng_s = Engine(local, hbm_budget=int(args.serve_budget_gb * 1e9))
+        extra["serving"] = with_clocks(local, SV.measure, eng_s, rate_hz=20.0, duration_s=args.serve_window,
+                                       warmup_s=args.serve_warmup)
+        eng_s.close()
+        extra["batched"] = with_clocks(local, B.measure, eng, n=args.batch_n, steps=3000)
+        extra["slab2d"] = with_clocks(local, measure_slab2d, eng)
+        if not args.no_large:
+            extra["large"] = with_clocks(local, L.run, eng=eng, peak_gbs=peak)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_baseline(spec, target_s=args.cpu_seconds)
+        cpu = cpu_baseline(spec)
     eng.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, "grid": list(spec.shape), "steps_per_sim": spec.nt,
-                       "nf": spec.nf, "parallelism": "replicas x%d" % ws,
-                       "l2": "inputs larger than L2 (%.0f MB device state per run > 126 MB)" %
-                             (spec.ncells * 4 * 9 / 1e6 + psi_elements(spec) * 4 / 1e6)},
+            "config": bench_config(spec, ws),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "k_y3_e (E half-step, one launch per time step)",
-                         "ms_per_launch": round(ms_e, 5), "algorithmic_bytes": alg["E"], "peak_kind": peak_kind,
-                         "h_half": {"kernel": "k_y3_h", "ms_per_launch": round(ms_h, 5),
-                                    "algorithmic_bytes": alg["H"], "achieved": round(achieved_h, 1),
-                                    "frac": round(achieved_h / peak, 4)},
-                         "ms_dft_fold_per_16_steps": round(ms_fold, 5)},
+                         "frac": round(achieved / peak, 4), "traffic": ncu_traffic(), "peak_kind": peak_kind,
+                         "kernel": "one time step: k_v3_e + k_v3_h, and k_fold once per 32 steps",
+                         "bytes_per_step": int(step_bytes), "ms_per_time_step": round(ms_ts, 5),
+                         "per_launch": {"k_v3_e": {"ms": round(ms_e, 5), "bytes": half["E"],
+                                                   "gbs": round(half["E"] / (ms_e * 1e-3) / 1e9, 1)},
+                                        "k_v3_h": {"ms": round(ms_h, 5), "bytes": half["H"],
+                                                   "gbs": round(half["H"] / (ms_h * 1e-3) / 1e9, 1)},
+                                        "k_fold_per_16_steps_ms": round(ms_fold, 5)}},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e, 3)},
             "gpu_launches": int(launches),
-            "batched": batched,
-            "serving": serving,
-            "slab2d": slab2d,
             "clocks": clk,
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    return 0
+
+
+NCU_CASES = ("strip3d", "rib_section", "large", "slab2d", "scatter", "zwave")
+
+
+def run_ncu_case(args):
+    """A fixed workload for profiler captures: one job, ``--case-steps``
+    steps, then exit.  strip3d is the benchmark grid (about 0.2 GB of device
+    state in FP32); rib_section the large run's 384 x 384 cross-section on a
+    256-cell guide (about 0.9 GB).  Captures that collect more than
+    gpu__time_duration.sum use one of these two with a single -k kernel and a
+    few launches; large (151 M cells, the large run itself), scatter and zwave
+    (the scattering-loss and wave-impedance runs at their reference settings,
+    75 M and 97 M cells) are for launch lists (gpu__time_duration.sum) only."""
+    from oidt_b200 import workloads as W
+    from oidt_b200.build import build
+    from oidt_b200.engine import Engine
+    build()
+    n = max(args.case_steps, 64)
+    if args.ncu_case == "strip3d":
+        spec = W.strip3d(**dict(WORKLOAD, steps=n))
+    elif args.ncu_case in ("rib_section", "large"):
+        from oidt_b200 import large as L
+        spec = L.large_spec(steps=n, shape=(384, 384, 256) if args.ncu_case == "rib_section" else L.SHAPE)
+    elif args.ncu_case == "scatter":
+        from oidt_b200 import scatter
+        cfg = scatter.config()
+        spec = scatter.build_spec(cfg, scatter.realization_profiles(cfg, 1)[0])
+    elif args.ncu_case == "zwave":
+        from oidt_b200 import zwave
+        spec = zwave.build_spec(zwave.config())
+    else:
+        spec = W.slab2d(steps=n)
+    eng = Engine(0)
+    job = eng.submit(spec, precision=np.dtype(args.precision), variant=args.variant, graphs=not args.no_graphs)
+    job.advance(args.case_steps).sync()
+    print("ran", args.case_steps, "steps of", args.ncu_case, spec.shape)
+    job.release()
+    eng.close()
     return 0
 
 
@@ -398,10 +500,20 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
-                    help="skip the batched-realization, served-mix and 2D slab measurements")
+                    help="skip the served-mix, batched-realization, 2D slab and large-run measurements")
     ap.add_argument("--batch-n", type=int, default=64, help="realizations in the batched-vs-plain measurement")
-    ap.add_argument("--serve-window", type=float, default=3.0, help="seconds of served-mix arrivals (20 jobs/s)")
+    ap.add_argument("--serve-window", type=float, default=60.0, help="seconds of served-mix arrivals (20 jobs/s)")
+    ap.add_argument("--serve-warmup", type=float, default=5.0, help="seconds of untimed served mix before it")
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0, help="HBM budget of the serving context")
+    ap.add_argument("--no-large", action="store_true", help="skip the 151 M-cell rib run")
+    ap.add_argument("--ncu-case", choices=NCU_CASES, help="run one fixed workload for a profiler capture and exit")
+    ap.add_argument("--case-steps", type=int, default=32)
+    ap.add_argument("--variant", default="vec", choices=("vec", "cell", "sweep"))
+    ap.add_argument("--no-graphs", action="store_true")
+    ap.add_argument("--precision", default="float32", choices=("float32", "float64"))
     args = ap.parse_args()
+    if args.ncu_case:
+        return run_ncu_case(args)
     ws, rank, local = dist_env()
     if args.impl == "reference":
         return run_reference(args, ws, rank, local)

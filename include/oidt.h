@@ -34,7 +34,7 @@ extern "C" {
 #define OIDT_ABI_VERSION 4  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe);
                               3: launch choices (reserved[2..3]), oidt_job_port_power;
                               4: oidt_job_read_dft_window_static, the vector launch form
-                                 (reserved[0] = 2) */
+                                 (reserved[0] = 2), oidt_job_set_wait_limit */
 
 /* status codes */
 #define OIDT_OK 0
@@ -233,6 +233,16 @@ int32_t oidt_job_release(oidt_ctx *ctx, uint64_t job);
  * same structure without another host-to-device copy.  The reference has no
  * counterpart (it starts a new process per simulation, fdtd_main.py:51-53). */
 int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job);
+
+/* Bound, in SM clock cycles, on each wait of the plane-sweep kernel
+ * (reserved[0] = 1) for a plane's tile loads; cycles <= 0 restores the
+ * default (4e9, about 2 s).  A wait that runs out marks the job failed --
+ * oidt_job_sync then returns OIDT_ERR_TIMEOUT -- and the kernel returns after
+ * the copies it has in flight have landed (those waits keep the default
+ * bound).  For tests of that failure path: a small bound makes the waits run
+ * out on loads that are merely in flight.  No counterpart in the reference
+ * (its kernels do not wait on one another). */
+int32_t oidt_job_set_wait_limit(oidt_ctx *ctx, uint64_t job, int64_t cycles);
 
 /* The context's compute stream (a cudaStream_t), so callers can order their
  * own work or record CUDA events around oidt_job_advance. */

@@ -544,6 +544,7 @@ struct Job {
   cudaEvent_t done = nullptr;                     // last enqueued work finished
   long long steps_enqueued = 0;
   bool busy = false;
+  long long wait_cycles = kWaitCycles;  // plane sweep: bound on its tile-load waits
 };
 
 constexpr int kAuxStreams = 64;  // a served request is two jobs; the mix keeps ~40 active
@@ -653,6 +654,7 @@ template <typename T> void fill_params(Job *J) {
     p.dx = (T)d.dx;
     p.rdx = (T)(1.0 / (double)p.dx);
     p.psx = p.psy = pl.psi_pitch;
+    p.wait_cycles = J->wait_cycles;
     for (auto fa : psi_pairs(d.mode))
       for (int sd = 0; sd < 2; ++sd) {
         const bool two = is_e(fa.first) && pl.nbuf == 2;
@@ -803,8 +805,8 @@ void y3_half(int rows, bool H, bool pdl, const Params<T> &p, int s, cudaStream_t
 }
 
 // Split of a 3D row between the vector form's roles: four-cell groups over
-// k in [kb + P, ke - P) rounded inward to multiples of 4, the rest one cell per
-// thread.
+// k in [kb + P, ke - P) rounded inward to multiples of 4 (vector role), the
+// other four-cell groups of the row (edge role).
 template <typename T> VecGeom vec_geom(const Params<T> &p) {
   VecGeom g;
   g.kz0 = (p.kb + p.P + 3) / 4 * 4;
@@ -821,7 +823,7 @@ template <typename T> VecGeom vec_geom(const Params<T> &p) {
 // blocks, of one x-plane per grid row.
 template <typename T, bool EXACT> void v3_half(bool H, bool pdl, const Params<T> &p, int s, cudaStream_t st) {
   const VecGeom g = vec_geom(p);
-  const long long nb_edge = ((long long)(p.je - p.jb) * g.nedge + kVecThreads - 1) / kVecThreads;
+  const long long nb_edge = ((long long)(p.je - p.jb) * (g.nedge / 4) + kVecThreads - 1) / kVecThreads;
   const dim3 grd((unsigned)(g.nb_vec + nb_edge), p.ie - p.ib), blk(kVecThreads);
   void (*kern)(Params<T>, VecGeom, int) = H ? k_v3_h<T, EXACT> : k_v3_e<T, EXACT>;
   if (pdl) launch_step_kernel(kern, grd, blk, 0, st, p, g, s);
@@ -1558,13 +1560,15 @@ int32_t oidt_job_read_dft_window_static(oidt_ctx *ctx, uint64_t job, int32_t por
     scratch = g_static_addr[ctx->device];
   }
   const double2 *acc = reinterpret_cast<const double2 *>(J->mem + J->pl.off_acc) + ((size_t)port * nc + comp) * J->d.nf * J->pl.plane;
+  // on the readout stream: read_common has waited for this job's work, and
+  // steps other jobs have queued on the compute stream do not delay the read
   const long long blocks = std::min<long long>((long long)(cells + 255) / 256, 148LL * 8);
-  k_gather_window<<<(unsigned)std::max(1LL, blocks), 256, 0, ctx->stream>>>(
+  k_gather_window<<<(unsigned)std::max(1LL, blocks), 256, 0, ctx->readout>>>(
       acc, static_cast<double2 *>(scratch), J->d.nf, J->pl.plane, is3 ? J->d.ny : 0, i0, wi, j0, wj);
   CU(ctx, cudaGetLastError());
   ctx->launches += 1;
-  CU(ctx, cudaMemcpyAsync(out, scratch, need * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  CU(ctx, cudaStreamSynchronize(ctx->stream));
+  CU(ctx, cudaMemcpyAsync(out, scratch, need * 8, cudaMemcpyDeviceToHost, ctx->readout));
+  CU(ctx, cudaStreamSynchronize(ctx->readout));
   return OIDT_OK;
 }
 
@@ -1678,6 +1682,25 @@ int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
   J->busy = true;
   J->steps_enqueued = 0;
   J->parity = 0;
+  return OIDT_OK;
+}
+
+int32_t oidt_job_set_wait_limit(oidt_ctx *ctx, uint64_t job, int64_t cycles) {
+  if (!ctx) return OIDT_ERR_INVALID;
+  std::lock_guard<std::mutex> g(ctx->mu);
+  Job *J = find(ctx, job);
+  if (!J) return fail(ctx, OIDT_ERR_NOTFOUND, "unknown job %llu", (unsigned long long)job);
+  CU(ctx, cudaSetDevice(ctx->device));
+  CU(ctx, cudaEventSynchronize(J->done));  // no launch holds the old parameters
+  J->wait_cycles = cycles > 0 ? (long long)cycles : kWaitCycles;
+  for (int b = 0; b < 2; ++b) {
+    J->pvf[b].wait_cycles = J->pcf[b].wait_cycles = J->wait_cycles;
+    J->pvd[b].wait_cycles = J->pcd[b].wait_cycles = J->wait_cycles;
+    if (J->graph[b]) {  // captured with the old parameters: capture again at next use
+      cudaGraphExecDestroy(J->graph[b]);
+      J->graph[b] = nullptr;
+    }
+  }
   return OIDT_OK;
 }
 

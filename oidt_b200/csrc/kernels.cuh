@@ -82,6 +82,7 @@ template <typename T> struct Params {
                          // nz (the reference layout) or nzp (16-byte rows, vector form)
   const void *tmap_f;    // plane sweep: 6 CUtensorMaps of f[] (device memory)
   const void *tmap_cb;   // plane sweep: 3 CUtensorMaps of cb[]
+  long long wait_cycles; // plane sweep: bound on each wait for a plane's tile loads
   int src_field;         // -1: none
   int slo[3], shi[3];
   const T *jsrc;

@@ -23,8 +23,11 @@
 //
 // TMA boxes start at z = floor4(z0 - 1) (16-byte aligned x-coordinate) and
 // y = y0 - 1; out-of-range rows/columns read as zero.  Waits on the TMA
-// mbarriers are bounded (kWaitCycles): on expiry the CTA records an error in
-// state[1], stops issuing, waits the same bound for copies in flight, returns.
+// mbarriers are bounded (p.wait_cycles, kWaitCycles unless a test lowers it):
+// on expiry the CTA records an error in state[1], stops issuing, waits for the
+// copies it has in flight (each wait bounded by kWaitCycles: every copy is a
+// valid load that lands) and returns, so nothing is written into its shared
+// memory after it exits.
 #pragma once
 #include <cuda.h>
 
@@ -187,14 +190,15 @@ __global__ void __launch_bounds__(TBY *TBZ, sizeof(T) == 4 ? 4 : 2)
     for (int a = 0; a < 3; ++a) tma_load_3d(dst + (6 + a) * BOXS, tmc + a * 128, zb, y0 - 1, xi, b);
   };
   // plane u lives in stage u % S and completes that stage's phase u / S
-  auto wait = [&](int k, unsigned parity) -> bool {
+  auto wait_for = [&](int k, unsigned parity, long long limit) -> bool {
     if (mbar_try_wait(bar + k, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar + k, parity)) {
-      if (clock64() - t0 > kWaitCycles) return false;
+      if (clock64() - t0 > limit) return false;
     }
     return true;
   };
+  auto wait = [&](int k, unsigned parity) -> bool { return wait_for(k, parity, p.wait_cycles); };
 
   if (tid == 0) {
     s_abort[0] = s_abort[1] = 0;
@@ -510,7 +514,7 @@ __global__ void __launch_bounds__(TBY *TBZ, sizeof(T) == 4 ? 4 : 2)
   if (aborted && tid == 0) {
     atomicExch(p.state + 1, 1);  // reported to the host by oidt_job_sync
     // copies issued after the failed one: bounded wait so none lands after exit
-    for (int v = s_failed; v < s_issued; ++v) (void)wait(v % S, (unsigned)((v / S) & 1));
+    for (int v = s_failed; v < s_issued; ++v) (void)wait_for(v % S, (unsigned)((v / S) & 1), kWaitCycles);
   }
 }
 

@@ -13,9 +13,10 @@
 //   component update ranges (only i = ib and j = jb leave a component out):
 //   no per-cell test runs in this role.  A plane is a flat list of (row,
 //   four-cell group) pairs, so no lane idles whatever nz is.
-// * edge role: every other cell (the z slabs and the rim, 9 % of the cells
-//   of a 256-cell guide with a 10-cell CPML), one per thread, through the
-//   per-cell code of kernels.cuh (y3_e_masked / y3_h_masked).
+// * edge role: every other four-cell group (the z slabs, the rim and the row
+//   padding: 9 % of the cells of a 256-cell guide with a 10-cell CPML), with
+//   each component's update range tested per cell and the z-slab psi read and
+//   written per cell.
 //
 // Per cell the arithmetic is the sequence of kernels.cuh's y3_e_compute /
 // y3_h_compute (the reference's fdtd_funcs.py:43-266 in its launch order):
@@ -33,6 +34,12 @@
 namespace oidt {
 
 constexpr int kVecThreads = 128;
+// Six resident blocks per SM (at most 80 registers a thread): the vector
+// role's loads in flight come from occupancy, and the edge role's longer code
+// would otherwise raise the whole kernel's register count (measured: with six
+// blocks C2 73.9 us and a 384 x 384 x 256 grid 0.612 ms per step, against 83.6
+// and 0.694 with the compiler's own 96-107 registers).
+constexpr int kVecBlocksPerSM = 6;
 
 template <typename T> struct V4 { T v[4]; };
 
@@ -77,20 +84,332 @@ template <typename T> __device__ __forceinline__ bool near_src(const Params<T> &
          k0 + nk > p.slo[2] - 1 && k0 < p.shi[2];
 }
 
-// Edge role: thread t of the plane's edge cells, one cell.
-template <typename T, bool EXACT, bool H>
-__device__ __forceinline__ void v3_edge(const Params<T> &p, const VecGeom &g, int i, int s) {
+// Edge role: four-cell groups k0 in [0, kz0) and [kz1, nzp) -- the z slabs,
+// the rim and the row padding -- with the update range of every component
+// tested per cell and the z-slab psi read and written per cell (all old
+// values of a group read before the first write).  Groups within one cell of
+// the source box run y3_e_cell / y3_h_cell per cell.
+template <typename T> __device__ __forceinline__ bool edge_group(const Params<T> &p, const VecGeom &g, int &j, int &k0) {
+  const int nge = g.nedge >> 2;
   const int t = (blockIdx.x - g.nb_vec) * kVecThreads + threadIdx.x;
-  if (t >= (p.je - p.jb) * g.nedge) return;
-  const int r = t / g.nedge, e = t - r * g.nedge;
-  const int j = p.jb + r, k = e < g.kz0 ? e : g.kz1 + (e - g.kz0);
-  if (k >= p.nz) return;
-  if (near_src(p, i, j, k, 1)) {
-    if (H) y3_h_cell<T, EXACT>(p, i, j, k, p.state[0] + s, s);
-    else y3_e_cell<T, EXACT>(p, i, j, k, p.state[0] + s, s);
-  } else {
-    if (H) y3_h_masked<T, EXACT>(p, i, j, k, s);
-    else y3_e_masked<T, EXACT>(p, i, j, k, s);
+  if (t >= (p.je - p.jb) * nge) return false;
+  const int r = t / nge, e4 = 4 * (t - r * nge);
+  j = p.jb + r;
+  k0 = e4 < g.kz0 ? e4 : g.kz1 + (e4 - g.kz0);
+  return true;
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void v3_edge_e(const Params<T> &p, const VecGeom &g, int i, int s) {
+  int j, k0;
+  if (!edge_group(p, g, j, k0)) return;
+  if (near_src(p, i, j, k0, 4)) {
+    for (int m = 0; m < 4; ++m)
+      if (k0 + m < p.nz) y3_e_cell<T, EXACT>(p, i, j, k0 + m, p.state[0] + s, s);
+    return;
+  }
+  using A = Ar<T, EXACT>;
+  const int P = p.P;
+  const bool iex = i > p.ib, jey = j > p.jb;
+  bool mex[4], mey[4], mez[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int k = k0 + m;
+    const bool kc = k >= p.kb && k < p.ke;
+    mex[m] = iex && kc;
+    mey[m] = jey && kc;
+    mez[m] = k > p.kb && k < p.ke;
+  }
+  const int sy = p.nzp;
+  const long long sx = (long long)p.ny * p.nzp, bi = (long long)i * sx;
+  const int o = j * sy + k0;
+  const T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
+  V4<T> Hx, Hy, Hz, Hzy, Hxy, Hzx, Hyx, C0, C1, C2, Ex, Ey, Ez, Rz, Kz;
+  ld4(Hx, hx + o);
+  ld4(Hy, hy + o);
+  ld4(Hz, hz + o);
+  ld4(Hzy, hz + (o + sy));
+  ld4(Hxy, hx + (o + sy));
+  ld4(Hzx, hz + sx + o);
+  ld4(Hyx, hy + sx + o);
+  const bool kn = k0 + 4 < p.nzp;  // the k + 1 neighbour of the last cell
+  const T hyk = kn ? __ldg(hy + (o + 4)) : T(0), hxk = kn ? __ldg(hx + (o + 4)) : T(0);
+  ld4(C0, p.cb[0] + bi + o);
+  ld4(C1, p.cb[1] + bi + o);
+  ld4(C2, p.cb[2] + bi + o);
+  T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
+  ldw4(Ex, ex + o);
+  ldw4(Ey, ey + o);
+  ldw4(Ez, ez + o);
+  ld4(Rz, p.rkd[2] + k0);
+  if (EXACT) ld4(Kz, p.kd[2] + k0);
+  const T rkx = p.rkd[0][i], rky = p.rkd[1][j];
+  const T kx = EXACT ? p.kd[0][i] : T(0), ky = EXACT ? p.kd[1][j] : T(0);
+  T e0[4], e1[4], e2[4], dzy[4], dyz[4], dxz[4], dzx[4], dyx[4], dxy[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const T hy1 = m < 3 ? Hy.v[m + 1] : hyk, hx1 = m < 3 ? Hx.v[m + 1] : hxk;
+    const T kz = EXACT ? Kz.v[m] : T(0);
+    dzy[m] = A::sub(Hzy.v[m], Hz.v[m]);
+    dyz[m] = A::sub(hy1, Hy.v[m]);
+    dxz[m] = A::sub(hx1, Hx.v[m]);
+    dzx[m] = A::sub(Hzx.v[m], Hz.v[m]);
+    dyx[m] = A::sub(Hyx.v[m], Hy.v[m]);
+    dxy[m] = A::sub(Hxy.v[m], Hx.v[m]);
+    e0[m] = A::add(Ex.v[m], A::mul(C0.v[m], A::sub(A::div(dzy[m], ky, rky), A::div(dyz[m], kz, Rz.v[m]))));
+    e1[m] = A::add(Ey.v[m], A::mul(C1.v[m], A::sub(A::div(dxz[m], kz, Rz.v[m]), A::div(dzx[m], kx, rkx))));
+    e2[m] = A::add(Ez.v[m], A::mul(C2.v[m], A::sub(A::div(dyx[m], kx, rkx), A::div(dxy[m], ky, rky))));
+  }
+  int d, side, q;
+  if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_ey_xinc, update_pml_ez_xinc
+    const long long oa = ((long long)d * p.ny + j) * p.psx + k0;
+    const T be = p.be[q], ce = p.ce[q];
+    T *const py = p.psi[EY][AX][side] + oa, *const pz = p.psi[EZ][AX][side] + oa;
+    V4<T> Py, Pz;
+    ldw4(Py, py);
+    ldw4(Pz, pz);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (mey[m]) {
+        Py.v[m] = A::add(A::mul(be, Py.v[m]), A::div(A::mul(ce, dzx[m]), p.dx, p.rdx));
+        e1[m] = A::sub(e1[m], A::mul(C1.v[m], Py.v[m]));
+      }
+      if (mez[m]) {
+        Pz.v[m] = A::add(A::mul(be, Pz.v[m]), A::div(A::mul(ce, dyx[m]), p.dx, p.rdx));
+        e2[m] = A::add(e2[m], A::mul(C2.v[m], Pz.v[m]));
+      }
+    }
+    st4(py, Py.v);
+    st4(pz, Pz.v);
+  }
+  if ((q = e_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_ex_yinc, update_pml_ez_yinc
+    const long long oa = ((long long)i * P + d) * p.psy + k0;
+    const T be = p.be[q], ce = p.ce[q];
+    T *const px = p.psi[EX][AY][side] + oa, *const pz = p.psi[EZ][AY][side] + oa;
+    V4<T> Px, Pz;
+    ldw4(Px, px);
+    ldw4(Pz, pz);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (mex[m]) {
+        Px.v[m] = A::add(A::mul(be, Px.v[m]), A::div(A::mul(ce, dzy[m]), p.dx, p.rdx));
+        e0[m] = A::add(e0[m], A::mul(C0.v[m], Px.v[m]));
+      }
+      if (mez[m]) {
+        Pz.v[m] = A::add(A::mul(be, Pz.v[m]), A::div(A::mul(ce, dxy[m]), p.dx, p.rdx));
+        e2[m] = A::sub(e2[m], A::mul(C2.v[m], Pz.v[m]));
+      }
+    }
+    st4(px, Px.v);
+    st4(pz, Pz.v);
+  }
+  // update_pml_ex_zinc, update_pml_ey_zinc: every old z-slab psi value of the
+  // group is read before the first is written
+  int qz[4], dz[4], sz[4];
+  T zx[4], zy[4];
+  const long long ob = ((long long)i * p.ny + j) * P;  // z-slab psi row (i, j)
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    dz[m] = 0;
+    sz[m] = 0;
+    qz[m] = mex[m] || mey[m] ? e_slab(k0 + m, p.kb, p.ke, P, dz[m], sz[m]) : -1;
+    zx[m] = qz[m] >= 0 && mex[m] ? p.psi[EX][AZ][sz[m]][ob + dz[m]] : T(0);
+    zy[m] = qz[m] >= 0 && mey[m] ? p.psi[EY][AZ][sz[m]][ob + dz[m]] : T(0);
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    if (qz[m] < 0) continue;
+    const T be = p.be[qz[m]], ce = p.ce[qz[m]];
+    if (mex[m]) {
+      zx[m] = A::add(A::mul(be, zx[m]), A::div(A::mul(ce, dyz[m]), p.dx, p.rdx));
+      p.psi[EX][AZ][sz[m]][ob + dz[m]] = zx[m];
+      e0[m] = A::sub(e0[m], A::mul(C0.v[m], zx[m]));
+    }
+    if (mey[m]) {
+      zy[m] = A::add(A::mul(be, zy[m]), A::div(A::mul(ce, dxz[m]), p.dx, p.rdx));
+      p.psi[EY][AZ][sz[m]][ob + dz[m]] = zy[m];
+      e1[m] = A::add(e1[m], A::mul(C1.v[m], zy[m]));
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {  // cells outside a component's range keep their value
+    e0[m] = mex[m] ? e0[m] : Ex.v[m];
+    e1[m] = mey[m] ? e1[m] : Ey.v[m];
+    e2[m] = mez[m] ? e2[m] : Ez.v[m];
+  }
+  st4(ex + o, e0);
+  st4(ey + o, e1);
+  st4(ez + o, e2);
+#pragma unroll
+  for (int pq = 0; pq < 2; ++pq) {
+    const int dm = p.port_pos[pq] - k0;
+    if ((unsigned)dm < 4u) {
+      const long long pc = (long long)i * p.ny + j;
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+        if (m == dm) {
+          if (mex[m]) capture(p, s, pq, 0, pc, e0[m]);
+          if (mey[m]) capture(p, s, pq, 1, pc, e1[m]);
+        }
+    }
+  }
+}
+
+template <typename T, bool EXACT>
+__device__ __forceinline__ void v3_edge_h(const Params<T> &p, const VecGeom &g, int i, int s) {
+  int j, k0;
+  if (!edge_group(p, g, j, k0)) return;
+  if (near_src(p, i, j, k0, 4)) {
+    for (int m = 0; m < 4; ++m)
+      if (k0 + m < p.nz) y3_h_cell<T, EXACT>(p, i, j, k0 + m, p.state[0] + s, s);
+    return;
+  }
+  using A = Ar<T, EXACT>;
+  const int P = p.P;
+  const bool ihy = i > p.ib, jhx = j > p.jb;
+  bool mhx[4], mhy[4], mhz[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int k = k0 + m;
+    const bool kc = k >= p.kb && k < p.ke, ko = k > p.kb && k < p.ke;
+    mhx[m] = jhx && ko;
+    mhy[m] = ihy && ko;
+    mhz[m] = ihy && jhx && kc;
+  }
+  const int sy = p.nzp;
+  const long long sx = (long long)p.ny * p.nzp, bi = (long long)i * sx;
+  const int o = j * sy + k0;
+  const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
+  V4<T> Ex, Ey, Ez, Ezy, Exy, Ezx, Eyx, Hx, Hy, Hz, Rz, Kz;
+  ld4(Ex, ex + o);
+  ld4(Ey, ey + o);
+  ld4(Ez, ez + o);
+  ld4(Ezy, ez + (o - sy));
+  ld4(Exy, ex + (o - sy));
+  ld4(Ezx, ez - sx + o);
+  ld4(Eyx, ey - sx + o);
+  const bool kp = k0 > 0;  // the k - 1 neighbour of the first cell
+  const T eyk = kp ? __ldg(ey + (o - 1)) : T(0), exk = kp ? __ldg(ex + (o - 1)) : T(0);
+  T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
+  ldw4(Hx, hx + o);
+  ldw4(Hy, hy + o);
+  ldw4(Hz, hz + o);
+  ld4(Rz, p.rkd[5] + k0);
+  if (EXACT) ld4(Kz, p.kd[5] + k0);
+  const T rkx = p.rkd[3][i], rky = p.rkd[4][j];
+  const T kx = EXACT ? p.kd[3][i] : T(0), ky = EXACT ? p.kd[4][j] : T(0);
+  const T db = p.db;
+  T h0[4], h1[4], h2[4], dyz[4], dzy[4], dzx[4], dxz[4], dxy[4], dyx[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const T ey1 = m > 0 ? Ey.v[m - 1] : eyk, ex1 = m > 0 ? Ex.v[m - 1] : exk;
+    const T kz = EXACT ? Kz.v[m] : T(0);
+    dyz[m] = A::sub(Ey.v[m], ey1);
+    dzy[m] = A::sub(Ez.v[m], Ezy.v[m]);
+    dzx[m] = A::sub(Ez.v[m], Ezx.v[m]);
+    dxz[m] = A::sub(Ex.v[m], ex1);
+    dxy[m] = A::sub(Ex.v[m], Exy.v[m]);
+    dyx[m] = A::sub(Ey.v[m], Eyx.v[m]);
+    h0[m] = A::add(Hx.v[m], A::mul(db, A::sub(A::div(dyz[m], kz, Rz.v[m]), A::div(dzy[m], ky, rky))));
+    h1[m] = A::add(Hy.v[m], A::mul(db, A::sub(A::div(dzx[m], kx, rkx), A::div(dxz[m], kz, Rz.v[m]))));
+    h2[m] = A::add(Hz.v[m], A::mul(db, A::sub(A::div(dxy[m], ky, rky), A::div(dyx[m], kx, rkx))));
+  }
+  int d, side, q;
+  if ((q = h_slab(i, p.ib, p.ie, P, d, side)) >= 0) {  // update_pml_hy_xinc, update_pml_hz_xinc
+    const long long oa = ((long long)d * p.ny + j) * p.psx + k0;
+    const T bh = p.bh[q], ch = p.ch[q];
+    T *const py = p.psi[HY][AX][side] + oa, *const pz = p.psi[HZ][AX][side] + oa;
+    V4<T> Py, Pz;
+    ldw4(Py, py);
+    ldw4(Pz, pz);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (mhy[m]) {
+        Py.v[m] = A::add(A::mul(bh, Py.v[m]), A::div(A::mul(ch, dzx[m]), p.dx, p.rdx));
+        h1[m] = A::add(h1[m], A::mul(db, Py.v[m]));
+      }
+      if (mhz[m]) {
+        Pz.v[m] = A::add(A::mul(bh, Pz.v[m]), A::div(A::mul(ch, dyx[m]), p.dx, p.rdx));
+        h2[m] = A::sub(h2[m], A::mul(db, Pz.v[m]));
+      }
+    }
+    st4(py, Py.v);
+    st4(pz, Pz.v);
+  }
+  if ((q = h_slab(j, p.jb, p.je, P, d, side)) >= 0) {  // update_pml_hx_yinc, update_pml_hz_yinc
+    const long long oa = ((long long)i * P + d) * p.psy + k0;
+    const T bh = p.bh[q], ch = p.ch[q];
+    T *const px = p.psi[HX][AY][side] + oa, *const pz = p.psi[HZ][AY][side] + oa;
+    V4<T> Px, Pz;
+    ldw4(Px, px);
+    ldw4(Pz, pz);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (mhx[m]) {
+        Px.v[m] = A::add(A::mul(bh, Px.v[m]), A::div(A::mul(ch, dzy[m]), p.dx, p.rdx));
+        h0[m] = A::sub(h0[m], A::mul(db, Px.v[m]));
+      }
+      if (mhz[m]) {
+        Pz.v[m] = A::add(A::mul(bh, Pz.v[m]), A::div(A::mul(ch, dxy[m]), p.dx, p.rdx));
+        h2[m] = A::add(h2[m], A::mul(db, Pz.v[m]));
+      }
+    }
+    st4(px, Px.v);
+    st4(pz, Pz.v);
+  }
+  // update_pml_hx_zinc, update_pml_hy_zinc: old values read before any write
+  int qz[4], dz[4], sz[4];
+  T zx[4], zy[4];
+  const long long ob = ((long long)i * p.ny + j) * P;  // z-slab psi row (i, j)
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    dz[m] = 0;
+    sz[m] = 0;
+    qz[m] = mhx[m] || mhy[m] ? h_slab(k0 + m, p.kb, p.ke, P, dz[m], sz[m]) : -1;
+    zx[m] = qz[m] >= 0 && mhx[m] ? p.psi[HX][AZ][sz[m]][ob + dz[m]] : T(0);
+    zy[m] = qz[m] >= 0 && mhy[m] ? p.psi[HY][AZ][sz[m]][ob + dz[m]] : T(0);
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    if (qz[m] < 0) continue;
+    const T bh = p.bh[qz[m]], ch = p.ch[qz[m]];
+    if (mhx[m]) {
+      zx[m] = A::add(A::mul(bh, zx[m]), A::div(A::mul(ch, dyz[m]), p.dx, p.rdx));
+      p.psi[HX][AZ][sz[m]][ob + dz[m]] = zx[m];
+      h0[m] = A::add(h0[m], A::mul(db, zx[m]));
+    }
+    if (mhy[m]) {
+      zy[m] = A::add(A::mul(bh, zy[m]), A::div(A::mul(ch, dxz[m]), p.dx, p.rdx));
+      p.psi[HY][AZ][sz[m]][ob + dz[m]] = zy[m];
+      h1[m] = A::sub(h1[m], A::mul(db, zy[m]));
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    h0[m] = mhx[m] ? h0[m] : Hx.v[m];
+    h1[m] = mhy[m] ? h1[m] : Hy.v[m];
+    h2[m] = mhz[m] ? h2[m] : Hz.v[m];
+  }
+  st4(hx + o, h0);
+  st4(hy + o, h1);
+  st4(hz + o, h2);
+#pragma unroll
+  for (int pq = 0; pq < 2; ++pq) {
+    const int dm = p.port_pos[pq] - k0;
+    if ((unsigned)(dm + 1) < 5u) {
+      const long long pc = (long long)i * p.ny + j;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        if (m == dm) {
+          if (mhx[m]) capture(p, s, pq, 2, pc, h0[m]);
+          if (mhy[m]) capture(p, s, pq, 4, pc, h1[m]);
+        }
+        if (m == dm + 1) {
+          if (mhx[m]) capture(p, s, pq, 3, pc, h0[m]);
+          if (mhy[m]) capture(p, s, pq, 5, pc, h1[m]);
+        }
+      }
+    }
   }
 }
 
@@ -100,11 +419,11 @@ __device__ __forceinline__ void v3_edge(const Params<T> &p, const VecGeom &g, in
 // then edge-role blocks, x-planes ib..ie-1).
 // ---------------------------------------------------------------------------
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(kVecThreads) k_v3_e(Params<T> p, VecGeom g, int s) {
+__global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_e(Params<T> p, VecGeom g, int s) {
   pdl_wait();
   const int i = p.ib + blockIdx.y;
   if ((int)blockIdx.x >= g.nb_vec) {
-    v3_edge<T, EXACT, false>(p, g, i, s);
+    v3_edge_e<T, EXACT>(p, g, i, s);
     return;
   }
   const int t = blockIdx.x * kVecThreads + threadIdx.x;
@@ -242,11 +561,11 @@ __global__ void __launch_bounds__(kVecThreads) k_v3_e(Params<T> p, VecGeom g, in
 // (still in L2) and ends on the planes the next E half-step reads first.
 // ---------------------------------------------------------------------------
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(kVecThreads) k_v3_h(Params<T> p, VecGeom g, int s) {
+__global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_h(Params<T> p, VecGeom g, int s) {
   pdl_wait();
   const int i = p.ie - 1 - blockIdx.y;
   if ((int)blockIdx.x >= g.nb_vec) {
-    v3_edge<T, EXACT, true>(p, g, i, s);
+    v3_edge_h<T, EXACT>(p, g, i, s);
     return;
   }
   const int t = blockIdx.x * kVecThreads + threadIdx.x;

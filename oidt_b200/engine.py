@@ -23,7 +23,8 @@ EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error",
            "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
            "oidt_job_query", "oidt_job_read_dft", "oidt_job_read_field", "oidt_job_write_field",
            "oidt_job_read_psi", "oidt_job_release", "oidt_job_reset", "oidt_ctx_stream", "oidt_job_profile",
-           "oidt_job_read_dft_window_static", "oidt_job_read_probe", "oidt_job_port_power")
+           "oidt_job_read_dft_window_static", "oidt_job_read_probe", "oidt_job_port_power",
+           "oidt_job_set_wait_limit")
 
 
 class OidtError(RuntimeError):
@@ -82,6 +83,7 @@ def load_library(path: str = LIB_PATH):
             "oidt_job_reset": ([vp, u64], i32),
             "oidt_ctx_stream": ([vp, C.POINTER(vp)], i32),
             "oidt_job_profile": ([vp, u64, i32, C.POINTER(C.c_float)], i32),
+            "oidt_job_set_wait_limit": ([vp, u64, C.c_int64], i32),
         }
         L.oidt_abi_version.argtypes, L.oidt_abi_version.restype = [], i32
         if L.oidt_abi_version() != ABI_VERSION:
@@ -132,14 +134,14 @@ class Engine:
         self._check(self.lib.oidt_stats_get(self.ctx, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
-    def job_bytes(self, spec: SimSpec, precision=None, ring_steps=0, variant: str = "cell", march_depth: int = 0) -> int:
+    def job_bytes(self, spec: SimSpec, precision=None, ring_steps=0, variant: str = "vec", march_depth: int = 0) -> int:
         d, keep = to_desc(spec, precision=precision, ring_steps=ring_steps, variant=variant, march_depth=march_depth)
         b = C.c_uint64()
         self._check(self.lib.oidt_job_bytes(C.byref(d), C.byref(b)))
         return b.value
 
     def submit(self, spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0,
-               variant: str = "cell", graphs: bool = True, rows: int = 0, march_depth: int = 0) -> "Job":
+               variant: str = "vec", graphs: bool = True, rows: int = 0, march_depth: int = 0) -> "Job":
         """Create a job (the H2D boundary).  ``variant``, ``rows``,
         ``march_depth`` and ``ring_steps`` choose how it is launched, never
         what it computes (``oidt_b200.tune`` picks them by measurement)."""
@@ -290,6 +292,12 @@ class Job:
         self.eng._check(self.eng.lib.oidt_job_profile(self.eng.ctx, self.id, nsteps, ms))
         self.steps += nsteps
         return tuple(float(v) for v in ms)
+
+    def set_wait_limit(self, cycles: int):
+        """Bound (SM cycles) on the plane-sweep kernel's waits for its tile
+        loads; 0 restores the default.  For tests of the failure path."""
+        self.eng._check(self.eng.lib.oidt_job_set_wait_limit(self.eng.ctx, self.id, int(cycles)))
+        return self
 
     def release(self):
         if not self.released:

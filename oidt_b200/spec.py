@@ -97,15 +97,15 @@ def power_window(spec: SimSpec):
     return tuple(w) if w else (spec.win_lo[1], spec.win_hi[1])
 
 
-def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "cell",
+def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "vec",
             graphs: bool = True, rows: int = 0, march_depth: int = 0):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
     ``keepalive`` must outlive the ``oidt_job_create`` call.
 
-    ``variant`` (3D only): 'cell' (default) -- the per-cell E-half / H-half
-    launches; 'vec' -- the same two half-steps with four cells per thread
-    along z and 16-byte accesses; 'sweep' -- one plane-sweep launch per step
-    (E and H fused, TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
+    ``variant`` (3D only): 'vec' (default) -- the E-half / H-half launches
+    with four cells per thread along z and 16-byte accesses; 'cell' -- the
+    same half-steps with one cell per thread; 'sweep' -- one plane-sweep
+    launch per step (E and H fused, TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
     launches every step directly instead of replaying K-step CUDA graphs.
     ``rows`` (3D per-cell form): tile rows of a block, 2, 4 or 8 (0 = 4);
     ``march_depth`` (3D plane sweep): x-planes per work item (0 = the

@@ -35,7 +35,7 @@ import numpy as np
 
 from .spec import SimSpec
 
-DEFAULT = {"variant": "cell", "rows": 0, "march_depth": 0}
+DEFAULT = {"variant": "vec", "rows": 0, "march_depth": 0}
 CANDIDATES = (
     {"variant": "vec", "rows": 0, "march_depth": 0},
     {"variant": "cell", "rows": 4, "march_depth": 0},
@@ -143,5 +143,5 @@ class Tuner:
         for key, v in sorted(self.table.items()):
             t = v["ms_per_step"]
             out[key] = {"choice": label(v["choice"]), "ms_per_step": t[label(v["choice"])],
-                        "default_ms_per_step": t.get(label(dict(DEFAULT, rows=4)))}
+                        "default_ms_per_step": t.get(label(DEFAULT))}
         return out

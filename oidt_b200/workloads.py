@@ -7,8 +7,8 @@ benchmark workloads are stated:
 
 * ``slab2d``   2D TMz symmetric slab (400 x 200 cells, 20 nm, 2000 steps)
 * ``strip3d``  3D silicon strip with rough sidewalls (256 x 128 x 128 cells
-               along x, 20 nm, 4000 steps; uneven batched grids; the 151 M
-               cell run at 15 nm)
+               along x, 20 nm, 4000 steps; uneven batched grids), or with
+               ``slab_y_nm`` an etched rib (the 151 M cell run at 15 nm)
 
 Axis convention is the reference's 3D one: z is the propagation axis and the
 contiguous array axis, x carries the roughened core faces and y the other
@@ -109,8 +109,9 @@ def slab2d(nx=400, ny=200, dx=20e-9, P=10, n_core=3.48, n_clad=1.44, core_cells=
 def strip3d(nx=128, ny=128, nz=256, dx=20e-9, P=10, n_core=3.48, n_clad=1.44, core_x_nm=220.0,
             core_y_nm=500.0, src_gap=10, port_gap=20, steps=4000, nf=41, lam=(1450.0, 1650.0),
             lam0=1550.0, bw=0.5, courant=0.99, sigma_nm=10.0, lc_nm=50.0, seed=0, rough=True,
-            source="TE", m_grade=3, kappa_max=5, alpha_max=0.05, precision=np.float32) -> SimSpec:
-    """3D strip along z with sidewall roughness on the x-faces.
+            source="TE", m_grade=3, kappa_max=5, alpha_max=0.05, precision=np.float32,
+            slab_y_nm=0.0) -> SimSpec:
+    """3D strip (or rib) along z with sidewall roughness on the x-faces.
 
     The core is centred; ``core_x_nm`` is its extent along x (the roughened
     faces, the reference's ``sgl_wg_height``) and ``core_y_nm`` along y (the
@@ -118,6 +119,12 @@ def strip3d(nx=128, ny=128, nz=256, dx=20e-9, P=10, n_core=3.48, n_clad=1.44, co
     sits ``src_gap`` cells inside the z-CPML, ports ``port_gap`` cells past the
     source and mirrored at the far end; roughness spans the guide between the
     ports.
+
+    ``slab_y_nm`` > 0 makes a rib: a core-index slab of that thickness along
+    y, level with the bottom of the core and spanning the whole x extent (into
+    the CPML, which absorbs its slab modes), under a ridge of ``core_x_nm``
+    by ``core_y_nm`` total height whose x-faces carry the roughness -- an
+    etched-rib silicon guide with rough rib sidewalls.
     """
     eps_bg = n_clad ** 2
     eps = eps_bg * EPS0
@@ -143,6 +150,10 @@ def strip3d(nx=128, ny=128, nz=256, dx=20e-9, P=10, n_core=3.48, n_clad=1.44, co
     jin = np.zeros(ny, dtype=bool)
     jin[by:by + cy] = True
     mask = face[:, None, :] & jin[None, :, None]
+    cs = 0
+    if slab_y_nm > 0:
+        cs = min(cy, max(1, int(round(slab_y_nm * 1e-9 / dx))))
+        mask[:, by:by + cs, :] = True
     eps_cell = eps * ((n_core ** 2 / eps_bg) * mask + 1 * ~mask)
     prec = np.float64
     ex, ey, ez = staggered_eps(eps_cell, prec, (0, 1, 2))
@@ -163,8 +174,8 @@ def strip3d(nx=128, ny=128, nz=256, dx=20e-9, P=10, n_core=3.48, n_clad=1.44, co
         src_field=FIELD_ID[fld], src_lo=slo, src_hi=shi,
         j_src=wave_packet(steps, dt, C0 / (lam0 * 1e-9), bw), port_pos=(p1, p2),
         win_lo=(P, P), win_hi=(nx - P, ny - P), freqs=freqs, twiddles=twiddles(freqs, dt, steps), nt=steps,
-        meta=dict(workload="strip3d", dt=dt, seed=seed, sigma_nm=sigma_nm, lc_nm=lc_nm, rough=rough,
-                  power_window=((P, nx - P), (P, ny - P)), core=(bx, by, cx, cy)))
+        meta=dict(workload="rib3d" if cs else "strip3d", dt=dt, seed=seed, sigma_nm=sigma_nm, lc_nm=lc_nm,
+                  rough=rough, power_window=((P, nx - P), (P, ny - P)), core=(bx, by, cx, cy), slab_cells=cs))
 
 
 def with_smooth(spec_kwargs: dict) -> dict:

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (read-only) and Numba:
 
-    python tests/golden/make_golden.py --ref /root/reference [--only CASE]
+    python tests/golden/make_golden.py --ref <reference checkout> [--only CASE]
 
 For every case this script runs the reference's own, unmodified
 ``fdtd_main.py`` (and ``extract_sparams.py``) from
@@ -487,7 +487,7 @@ def copy_touchstone_examples(ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference checkout (read only)")
     ap.add_argument("--only", nargs="*")
     a = ap.parse_args()
     cs = cases(a.ref)

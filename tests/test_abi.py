@@ -67,7 +67,7 @@ def test_line_probe_descriptor_without_device():
     assert lib.oidt_job_bytes(ctypes.byref(d), ctypes.byref(b0)) == 0
     spec.meta["probe"] = (9, 20)
     d, keep = to_desc(spec)
-    assert list(d.probe) == [1, 9, 20] and list(d.reserved) == [0, 0, 0, 0]
+    assert list(d.probe) == [1, 9, 20] and list(d.reserved) == [2, 0, 0, 0]  # the vector launch form
     assert lib.oidt_job_bytes(ctypes.byref(d), ctypes.byref(b1)) == 0
     assert b1.value - b0.value >= 4 * 30 * 20 * 4  # float32 record [4][nt][nx]
     for bad in ((1, 18, 20), (1, 9, 39), (1, -1, 20), (2, 9, 20), (0, 9, 20)):

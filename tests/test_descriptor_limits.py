@@ -110,6 +110,7 @@ def test_plane_offsets_limit(lib):
     holds 2^31 or more elements are refused, and one just below is sized.
     Only host planning runs here; nothing is allocated."""
     d, keep = _d3()
+    d.reserved[0] = 0  # the per-cell form: psi rows of nz cells
     P = d.num_cpml
     for ny, nz, ok in ((46341, 46344, False),   # the plane itself
                        (23171, 23171, False),   # P x ny x nz just above 2^31 - 1
@@ -124,3 +125,21 @@ def test_plane_offsets_limit(lib):
             assert rc == 0 and b > ny * nz * 4 * 9 * d.nx
         else:
             assert rc == INVALID
+
+
+def test_vector_form_pitched_slab_limit(lib):
+    """The vector form keeps x- and y-slab psi rows padded to nzp cells, so
+    its limit is P x ny x nzp < 2^31: a grid the per-cell form still takes
+    (P ny nz just below the limit, nz not a multiple of 4) is refused."""
+    d, keep = _d3()
+    P = d.num_cpml
+    ny, nz = 23170, 23170  # nzp = 23172
+    d.ny, d.nz = ny, nz
+    d.je, d.ke = ny - 2, nz - 2
+    d.win_hi[1] = ny - 5
+    d.port_pos[0], d.port_pos[1] = 10, nz - 10
+    assert P * ny * nz < 2 ** 31 - 1 < P * ny * 23172
+    d.reserved[0] = 0
+    assert _bytes(lib, d)[0] == 0
+    d.reserved[0] = 2
+    assert _bytes(lib, d)[0] == INVALID

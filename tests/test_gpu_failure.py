@@ -73,3 +73,35 @@ def test_budget_refusal_keeps_the_context_usable():
     b.run().sync()
     b.release()
     eng.close()
+
+
+def test_sweep_tile_wait_expiry_is_reported_and_recoverable():
+    """The plane-sweep kernel's waits for its tile loads are bounded in the
+    kernel.  With a bound of one cycle they run out on loads that are merely
+    in flight; every CTA that gives up waits (with the default bound) for the
+    copies it issued before it returns, so nothing lands in its shared memory
+    afterwards.  oidt_job_sync reports the expiry as OIDT_ERR_TIMEOUT; the
+    context and, after a reset with the default bound, the job itself run as
+    before."""
+    eng = Engine(0)
+    spec = _spec(steps=64)
+    ref = eng.submit(spec, variant="sweep")
+    ref.advance(16).sync()
+    want = {f: ref.field(f) for f in ("EY", "HX")}
+    ref.release()
+
+    job = eng.submit(spec, variant="sweep")
+    job.set_wait_limit(1)
+    job.advance(16)
+    with pytest.raises(TimeoutError_, match="bounded wait"):
+        job.sync(60000)
+    other = eng.submit(spec, variant="sweep")  # the context still works
+    other.advance(16).sync(60000)
+    for f, v in want.items():
+        np.testing.assert_array_equal(other.field(f), v)
+    other.release()
+    job.set_wait_limit(0).reset().advance(16).sync(60000)  # default bound: the job recovers
+    for f, v in want.items():
+        np.testing.assert_array_equal(job.field(f), v)
+    job.release()
+    eng.close()

@@ -12,8 +12,12 @@ class FakeSpec:
         self.nt, self.bytes, self.mode, self.shape = nt, bytes_, mode, shape
         self.ncells = int(np.prod(shape))
         self.nf = 2
-        self.meta = {"power_window": (2, 28)}
-        self.win_lo, self.win_hi = (0, 2), (1, 28)
+        if mode == "yee3d":
+            self.meta = {"power_window": ((2, shape[0] - 2), (2, shape[1] - 2))}
+            self.win_lo, self.win_hi = (2, 2), (shape[0] - 2, shape[1] - 2)
+        else:
+            self.meta = {"power_window": (2, 28)}
+            self.win_lo, self.win_hi = (0, 2), (1, 28)
 
 
 class FakeJob:
@@ -137,3 +141,65 @@ def test_fair_share_groups_share_launches():
     batches = [e for e in eng.log if e[0] == "batch"]
     assert batches and all(n_jobs == 3 and n == 32 for _, n_jobs, n in batches)
     assert sum(n for _, _, n in batches) == 320
+
+
+def test_small_first_large_fifo_with_cap():
+    """Small requests (at most small_cells cells) are admitted as they arrive;
+    large ones first-come, first-served, at most max_large active at once --
+    later large requests wait even when memory allows, small ones never wait
+    behind them."""
+    eng = FakeEngine(budget=10 ** 9)
+    big = lambda: FakeSpec(nt=640, bytes_=1, mode="yee3d", shape=(20, 20, 20))  # 8000 cells
+    small = lambda: FakeSpec(nt=64, bytes_=1)                                   # 1200 cells
+    reqs = [Request(k, 0.0, big(), meta={"kind": "3d"}) for k in range(4)]
+    reqs += [Request(4 + k, 0.0, small(), meta={"kind": "2d"}) for k in range(3)]
+    srv = Server(eng, tick=64, small_cells=5000, max_large=2)
+    admitted = []
+    orig = srv._admit
+
+    def record(req, now):
+        ok = orig(req, now)
+        if ok:
+            admitted.append((req.rid, len([e for e in srv.active if not srv.is_small(e[0])])))
+        return ok
+    srv._admit = record
+    res = srv.run(reqs, realtime=False, depth=1)
+    assert sorted(r.rid for r in res) == list(range(7))
+    order = [rid for rid, _ in admitted]
+    assert order[:5] == [0, 1, 4, 5, 6]            # two large, then every small one at once
+    assert max(n for _, n in admitted) <= 2         # never more than max_large large jobs
+    assert order.index(2) < order.index(3)          # large ones in arrival order
+    assert srv.refused == 0                          # the cap, not the budget, held them back
+    by = {r.rid: r for r in res}
+    assert all(by[k].kind == ("3d" if k < 4 else "2d") and by[k].wait >= 0 for k in range(7))
+
+
+def test_requests_built_on_arrival():
+    """A request that carries a builder is built by the worker pool once it
+    has arrived, admitted when built, and its host arrays are dropped once the
+    job holds them; the served results equal those of prebuilt requests."""
+    def mk(k):
+        return FakeSpec(nt=96 + 32 * k, bytes_=1)
+
+    class Spec(FakeSpec):
+        def __init__(self, *a, **kw):
+            super().__init__(*a, **kw)
+            self.cb, self.kdx, self.twiddles = {"z": np.ones(3)}, {"xe": np.ones(3)}, (np.ones(2),)
+            self.be = self.ce = self.bh = self.ch = self.j_src = np.ones(2)
+
+    built = []
+
+    def builder(k):
+        def b():
+            built.append(k)
+            return Spec(nt=96 + 32 * k, bytes_=1), None
+        return b
+    eng = FakeEngine(budget=10 ** 9)
+    reqs = [Request(k, 0.0, meta={"kind": "2d", "cells": 1200}, build=builder(k)) for k in range(4)]
+    res = Server(eng, tick=32).run(reqs, realtime=False, workers=2)
+    assert sorted(built) == [0, 1, 2, 3] and sorted(r.rid for r in res) == [0, 1, 2, 3]
+    assert all(q.spec.cb == {} and q.spec.j_src is None for q in reqs)  # arrays dropped after admission
+    assert all(j.steps == j.spec.nt for j in eng.jobs)
+    ref = Server(FakeEngine(budget=10 ** 9), tick=32).run([Request(k, 0.0, mk(k)) for k in range(4)],
+                                                          realtime=False)
+    assert {r.rid: r.steps for r in res} == {r.rid: r.steps for r in ref}

@@ -27,13 +27,13 @@ def test_descriptor_launch_choices_validated_on_host():
     from oidt_b200.spec import to_desc
     lib = load_library()
     spec = _strip()
-    rc, base = _bytes(lib, to_desc(spec)[0])
+    rc, base = _bytes(lib, to_desc(spec, variant="cell")[0])
     assert rc == 0
     for rows in (2, 4, 8):  # tile rows change launches, not memory
-        d, keep = to_desc(spec, rows=rows)
+        d, keep = to_desc(spec, variant="cell", rows=rows)
         assert _bytes(lib, d) == (0, base)
     for rows in (1, 3, 16, -2):
-        d, keep = to_desc(spec, rows=rows)
+        d, keep = to_desc(spec, variant="cell", rows=rows)
         assert _bytes(lib, d)[0] == -1, rows
     d, keep = to_desc(spec, variant="sweep", rows=4)  # rows belong to the per-cell form
     assert _bytes(lib, d)[0] == -1
@@ -97,7 +97,7 @@ def test_tuner_picks_fastest_and_caches_per_shape(tmp_path):
     assert t2.choose(a, np.float32) == c and t2.calls == []
     s = t2.summary()
     key = tune.shape_key(a, np.float32, "fast", 32)
-    assert s[key]["choice"] == "cell/rows8" and s[key]["default_ms_per_step"] == TIMES["cell/rows4"]
+    assert s[key]["choice"] == "cell/rows8" and s[key]["default_ms_per_step"] == TIMES["vec"]
 
 
 def test_tuning_needs_enough_steps():
