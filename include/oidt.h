@@ -33,8 +33,9 @@ extern "C" {
 
 #define OIDT_ABI_VERSION 4  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe);
                               3: launch choices (reserved[2..3]), oidt_job_port_power;
-                              4: oidt_job_read_dft_window_static, the vector launch form
-                                 (reserved[0] = 2), oidt_job_set_wait_limit */
+                              4: oidt_job_read_dft_window_static, the vector and ordered
+                                 launch forms (reserved[0] = 2, 3), oidt_job_set_wait_limit,
+                                 the material index (mat_idx, mat_tab, nmat) */
 
 /* status codes */
 #define OIDT_OK 0
@@ -104,7 +105,9 @@ typedef struct oidt_job_desc {
   /* reserved[0]: 3D launch form, 0 = per-cell E-half / H-half launches,
    *              1 = plane sweep (one launch per step),
    *              2 = vector form: the E-half / H-half launches with four
-   *                  cells per thread along z and 16-byte accesses;
+   *                  cells per thread along z and 16-byte accesses,
+   *              3 = ordered form: the vector form's code in one launch per
+   *                  step, E and H half-steps ordered plane by plane;
    * reserved[1]: 1 = launch every step directly (no CUDA-graph replay);
    * reserved[2]: 3D per-cell form only: rows of a block's 32 x rows tile,
    *              2, 4 or 8 (0 = 4);
@@ -120,6 +123,18 @@ typedef struct oidt_job_desc {
    * z, z+1; Hy over (x, x+1) x (z, z+1); Hz over (x, x+1) x (y, y+1), at
    * y = probe[1], z = probe[2].  probe[0] = 0: no probe (probe[1..2] 0). */
   int32_t probe[3];
+  /* 3D only, optional: the dt/eps grids as a material index.  With mat_idx
+   * != NULL every cell's (CBX, CBY, CBZ) is mat_tab[mat_idx[cell]]:
+   * mat_idx [nx][ny][nz] bytes (C order), mat_tab [nmat][3] values in the
+   * job's precision, 1 <= nmat <= 256; cb[] is not read (NULL allowed).  The
+   * engine expands the grids on the device for the forms that read them; the
+   * vector form reads the index (1 byte per cell instead of three values).
+   * Results equal those of the expanded grids passed in cb[].  NULL: none
+   * (nmat 0).  No counterpart in the reference, whose CB arrays are built
+   * from its foreground mask (fdtd_main.py:86-118 (3D)). */
+  const uint8_t *mat_idx;
+  const void *mat_tab;
+  int32_t nmat;
 } oidt_job_desc;
 
 typedef struct oidt_stats {

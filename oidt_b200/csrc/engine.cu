@@ -53,7 +53,7 @@ constexpr int kBlock3Z = 32, kRowsDefault = 4;  // 3D per-cell tile: 32 (k) x ro
 constexpr int kBlock2 = 128;
 constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
 constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread box
-constexpr int kVariantCell = 0, kVariantSweep = 1, kVariantVec = 2;  // oidt_job_desc.reserved[0]
+constexpr int kVariantCell = 0, kVariantSweep = 1, kVariantVec = 2, kVariantWave = 3;  // oidt_job_desc.reserved[0]
 
 // ---------------------------------------------------------------------------
 // Line probe (wave-impedance recording): after every step, colocated Ey, Ez,
@@ -325,6 +325,9 @@ struct JobPlan {
   size_t off_psi[2][6][3][2];
   size_t off_jsrc, off_tw[4], off_ring, off_acc, off_state, off_tmaps, off_items;
   size_t off_probe, probe_bytes;  // line probe [4][nt][nx] (probe_bytes = 0: none)
+  size_t off_mat, off_mtab;       // material index [nx][ny][nzp] and table [256][4] (3D, optional)
+  bool mat;
+  size_t off_wave;                // ordered form: ticket counter (8 B) and E-block counts per plane
   size_t off_pow;                 // port power [nf] complex float64
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
@@ -398,6 +401,28 @@ int choose_chunk(const oidt_job_desc *d, int slots) {
 
 int g_sweep_slots = 0;  // SMs x resident sweep CTAs (set at context creation)
 
+// Split of a 3D row between the vector form's roles: four-cell groups over
+// k in [kb + P, ke - P) rounded inward to multiples of 4 (vector role), the
+// other four-cell groups of the row (edge role).
+VecGeom vec_geom_of(int kb, int ke, int P, int jb, int je, int nzp) {
+  VecGeom g;
+  g.kz0 = (kb + P + 3) / 4 * 4;
+  g.kz1 = (ke - P) / 4 * 4;
+  if (g.kz1 <= g.kz0) g.kz0 = g.kz1 = nzp;  // no z-clean group: every cell in the edge role
+  g.nvc = (g.kz1 - g.kz0) / 4;
+  g.nedge = g.kz0 + (nzp - g.kz1);
+  const long long rows = je - jb;
+  g.nb_vec = (int)((rows * g.nvc + kVecThreads - 1) / kVecThreads);
+  return g;
+}
+int vec_edge_blocks(const VecGeom &g, int jb, int je) {
+  return (int)(((long long)(je - jb) * (g.nedge / 4) + kVecThreads - 1) / kVecThreads);
+}
+long long vec_blocks_per_plane(const oidt_job_desc *d, int nzp) {
+  const VecGeom g = vec_geom_of(d->kb, d->ke, d->num_cpml, d->jb, d->je, nzp);
+  return (long long)g.nb_vec + vec_edge_blocks(g, d->jb, d->je);
+}
+
 int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   auto bad = [&](const char *m) { if (why) *why = m; return OIDT_ERR_INVALID; };
   if (!d) return bad("null descriptor");
@@ -418,8 +443,12 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   if (d->nt < 1 || d->nf < 1) return bad("nt and nf must be >= 1");
   if (!d->j_src || !d->cos_e || !d->sin_e || !d->cos_h || !d->sin_h || !d->be || !d->ce || !d->bh || !d->ch)
     return bad("missing source, twiddle or CPML arrays");
-  for (int c : cb_of(d->mode))
-    if (!d->cb[c]) return bad("missing cb array");
+  const bool mat = d->mat_idx || d->mat_tab || d->nmat;
+  if (mat && (!is3 || !d->mat_idx || !d->mat_tab || d->nmat < 1 || d->nmat > 256))
+    return bad("material index: 3D only, with mat_idx, mat_tab and 1 <= nmat <= 256");
+  if (!mat)
+    for (int c : cb_of(d->mode))
+      if (!d->cb[c]) return bad("missing cb array");
   for (int a = 0; a < 6; ++a)
     if (!d->kdx[a] && (is3 || (a != 2 && a != 5))) return bad("missing kappa*dx array");
   const int nalong = is3 ? d->nz : d->nx;
@@ -452,8 +481,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   } else if (d->probe[1] != 0 || d->probe[2] != 0) {
     return bad("probe[1..2] must be 0 without a probe");
   }
-  if (d->reserved[0] != kVariantCell && d->reserved[0] != kVariantSweep && d->reserved[0] != kVariantVec)
-    return bad("reserved[0]: launch form 0, 1 or 2");
+  if (d->reserved[0] < kVariantCell || d->reserved[0] > kVariantWave) return bad("reserved[0]: launch form 0 to 3");
   if (d->reserved[1] != 0 && d->reserved[1] != 1) return bad("reserved[1]: 0 or 1");
   const int variant = is3 ? d->reserved[0] : kVariantCell;
   const int rows = d->reserved[2] == 0 ? kRowsDefault : d->reserved[2];
@@ -470,8 +498,13 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   if (K > 4096) return bad("ring_steps too large");
   if (variant == kVariantSweep && (K & 1)) ++K;  // graphs of the sweep end on the parity they start
   const int nbuf = variant == kVariantSweep ? 2 : 1;
-  const int psi_pitch = variant == kVariantVec ? nzp : d->nz;
-  if (variant == kVariantVec) {  // 32-bit row offsets of the pitched slabs; x-planes on grid.y
+  const bool vec_rows = variant == kVariantVec || variant == kVariantWave;  // the vector form's kernels
+  const int psi_pitch = vec_rows ? nzp : d->nz;
+  if (variant == kVariantWave) {  // block counts per plane and step stay in 32-bit counters
+    const long long nb = vec_blocks_per_plane(d, nzp);
+    if ((long long)(d->nt + 1) * nb > 0x7fffffffLL) return bad("ordered form: nt x blocks per plane >= 2^31");
+  }
+  if (vec_rows) {  // 32-bit row offsets of the pitched slabs; x-planes on grid.y
     const long long lim = 0x7fffffffLL;
     if ((long long)P * d->ny * nzp > lim || (long long)d->nx * P * nzp > lim)
       return bad("grid too large: a pitched CPML slab holds 2^31 or more elements");
@@ -503,6 +536,12 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->off_acc = L.take((size_t)2 * ncomp_of(d->mode) * d->nf * plane * 16);
   pl->off_state = L.take(64);
   pl->off_pow = L.take((size_t)d->nf * 16);
+  if (mat) {
+    pl->mat = true;
+    pl->off_mat = L.take((size_t)N);
+    pl->off_mtab = L.take((size_t)256 * 4 * esz);
+  }
+  if (variant == kVariantWave) pl->off_wave = L.take(8 + (size_t)4 * (d->ie - d->ib));
   if (d->probe[0] == 1) {
     pl->probe_bytes = (size_t)4 * d->nt * d->nx * esz;
     pl->off_probe = L.take(pl->probe_bytes);
@@ -624,6 +663,17 @@ bool encode_map(CUtensorMap *m, void *base, int esz, int nzp, int ny, int nx) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// dt/eps grids of a job created with a material index: cb[c][cell] =
+// mtab[mat[cell]][c] for k < nz (the row padding stays zero).
+template <typename T> __global__ void k_mat_expand(Params<T> p) {
+  const long long n = (long long)p.nx * p.ny * p.nzp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    if (t % p.nzp >= p.nz) continue;
+    const T *e = p.mtab + 4 * (int)p.mat[t];
+    for (int c = 0; c < 3; ++c) const_cast<T *>(p.cb[c])[t] = e[c];
+  }
+}
+
 template <typename T> void fill_params(Job *J) {
   const oidt_job_desc &d = J->d;
   const JobPlan &pl = J->pl;
@@ -641,6 +691,8 @@ template <typename T> void fill_params(Job *J) {
       p.fn[f] = reinterpret_cast<T *>(m + pl.off_f[pl.nbuf == 2 ? bb ^ 1 : 0][f]);
     }
     for (int c : cb_of(d.mode)) p.cb[c] = reinterpret_cast<const T *>(m + pl.off_cb[c]);
+    p.mat = pl.mat ? m + pl.off_mat : nullptr;
+    p.mtab = pl.mat ? reinterpret_cast<const T *>(m + pl.off_mtab) : nullptr;
     for (int a = 0; a < 6; ++a) {
       if (d.mode != OIDT_MODE_YEE3D && (a == 2 || a == 5)) continue;
       p.kd[a] = reinterpret_cast<const T *>(m + pl.off_kd[a]);
@@ -721,9 +773,24 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
   unsigned char *m = J->mem;
   cudaStream_t st = ctx->upload;
   CU(ctx, cudaMemsetAsync(m, 0, pl.total, st));
-  for (int c : cb_of(d.mode)) {
-    int rc = copy_grid_h2d(ctx, J, m + pl.off_cb[c], d.cb[c], st);
-    if (rc) return rc;
+  std::vector<T> tab;
+  if (pl.mat) {  // the index (pitched like the grids) and its table; the grids are expanded below
+    const size_t row = d.nz, rows = (size_t)d.nx * d.ny;
+    const uint8_t *idx = d.mat_idx;
+    uint8_t hi = 0;
+    for (size_t q = 0; q < row * rows; ++q) hi = std::max(hi, idx[q]);
+    if (hi >= d.nmat) return fail(ctx, OIDT_ERR_INVALID, "material index %d >= nmat %d", (int)hi, d.nmat);
+    CU(ctx, cudaMemcpy2DAsync(m + pl.off_mat, pl.nzp, idx, row, row, rows, cudaMemcpyHostToDevice, st));
+    tab.assign((size_t)256 * 4, T(0));
+    const T *src = static_cast<const T *>(d.mat_tab);
+    for (int q = 0; q < d.nmat; ++q)
+      for (int c = 0; c < 3; ++c) tab[(size_t)q * 4 + c] = src[(size_t)q * 3 + c];
+    CU(ctx, cudaMemcpyAsync(m + pl.off_mtab, tab.data(), tab.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  } else {
+    for (int c : cb_of(d.mode)) {
+      int rc = copy_grid_h2d(ctx, J, m + pl.off_cb[c], d.cb[c], st);
+      if (rc) return rc;
+    }
   }
   const int dims[3] = {d.nx, d.ny, d.nz};
   std::vector<T> rk;
@@ -747,6 +814,15 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
   for (int t = 0; t < 4; ++t)
     CU(ctx, cudaMemcpyAsync(m + pl.off_tw[t], tw[t], (size_t)d.nf * d.nt * 8, cudaMemcpyHostToDevice, st));
   fill_params<T>(J);
+  if (pl.mat) {  // dt/eps grids from the index, for the forms and cells that read them
+    const Params<T> &p = cells<T>(J)[0];
+    const long long n = (long long)d.nx * d.ny * pl.nzp;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_mat_expand<T><<<blocks, 256, 0, st>>>(p);
+    CU(ctx, cudaGetLastError());
+    ctx->launches += 1;
+    CU(ctx, cudaStreamSynchronize(st));  // tab is a host temporary
+  }
   if (pl.variant == kVariantSweep) {
     std::vector<CUtensorMap> maps(15);
     for (int b = 0; b < 2; ++b)
@@ -804,30 +880,30 @@ void y3_half(int rows, bool H, bool pdl, const Params<T> &p, int s, cudaStream_t
   else y3_half_by<T, EXACT, 4>(H, pdl, p, s, st);
 }
 
-// Split of a 3D row between the vector form's roles: four-cell groups over
-// k in [kb + P, ke - P) rounded inward to multiples of 4 (vector role), the
-// other four-cell groups of the row (edge role).
-template <typename T> VecGeom vec_geom(const Params<T> &p) {
-  VecGeom g;
-  g.kz0 = (p.kb + p.P + 3) / 4 * 4;
-  g.kz1 = (p.ke - p.P) / 4 * 4;
-  if (g.kz1 <= g.kz0) g.kz0 = g.kz1 = p.nzp;  // no z-clean group: every cell in the edge role
-  g.nvc = (g.kz1 - g.kz0) / 4;
-  g.nedge = g.kz0 + (p.nzp - g.kz1);
-  const long long rows = p.je - p.jb;
-  g.nb_vec = (int)((rows * g.nvc + kVecThreads - 1) / kVecThreads);
-  return g;
-}
+template <typename T> VecGeom vec_geom(const Params<T> &p) { return vec_geom_of(p.kb, p.ke, p.P, p.jb, p.je, p.nzp); }
 
 // One 3D vector-form half-step: the vector-role blocks, then the edge-role
 // blocks, of one x-plane per grid row.
 template <typename T, bool EXACT> void v3_half(bool H, bool pdl, const Params<T> &p, int s, cudaStream_t st) {
   const VecGeom g = vec_geom(p);
-  const long long nb_edge = ((long long)(p.je - p.jb) * (g.nedge / 4) + kVecThreads - 1) / kVecThreads;
+  const long long nb_edge = vec_edge_blocks(g, p.jb, p.je);
   const dim3 grd((unsigned)(g.nb_vec + nb_edge), p.ie - p.ib), blk(kVecThreads);
   void (*kern)(Params<T>, VecGeom, int) = H ? k_v3_h<T, EXACT> : k_v3_e<T, EXACT>;
   if (pdl) launch_step_kernel(kern, grd, blk, 0, st, p, g, s);
   else kern<<<grd, blk, 0, st>>>(p, g, s);
+}
+
+// One time step of the ordered form: both half-steps, plane by plane, in one
+// launch of 2 (ie - ib) blocks per plane and half-step (k_v3_wave).
+template <typename T, bool EXACT> void v3_wave(Job *J, bool pdl, const Params<T> &p, int s, cudaStream_t st) {
+  const VecGeom g = vec_geom(p);
+  WaveArgs w;
+  w.ticket = reinterpret_cast<unsigned long long *>(J->mem + J->pl.off_wave);
+  w.done = reinterpret_cast<int *>(J->mem + J->pl.off_wave + 8);
+  w.nb = g.nb_vec + vec_edge_blocks(g, p.jb, p.je);
+  const dim3 grd((unsigned)(2LL * (p.ie - p.ib) * w.nb)), blk(kVecThreads);
+  if (pdl) launch_step_kernel(k_v3_wave<T, EXACT>, grd, blk, 0, st, p, g, w, s);
+  else k_v3_wave<T, EXACT><<<grd, blk, 0, st>>>(p, g, w, s);
 }
 
 template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, EYB, EZB, ST>(); }
@@ -870,6 +946,12 @@ template <typename T, bool EXACT> void launch_step(oidt_ctx *ctx, Job *J, int s,
     return;
   }
   Params<T> &p = cells<T>(J)[par];
+  if (J->pl.variant == kVariantWave) {
+    v3_wave<T, EXACT>(J, true, p, s, st);
+    ctx->launches += 1;
+    if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par, st);
+    return;
+  }
   if (J->pl.variant == kVariantVec) {
     v3_half<T, EXACT>(false, true, p, s, st);
     v3_half<T, EXACT>(true, true, p, s, st);
@@ -1053,6 +1135,16 @@ template <typename T, bool EXACT> int profile_t(oidt_ctx *ctx, Job *J, int nstep
       continue;
     }
     Params<T> &p = cells<T>(J)[par];
+    if (J->pl.variant == kVariantWave) {  // one launch per step: reported as the E half, H half = 0
+      cudaEventRecord(ev[q++], st);
+      v3_wave<T, EXACT>(J, false, p, s, st);
+      cudaEventRecord(ev[q++], st);
+      cudaEventRecord(ev[q++], st);
+      cudaEventRecord(ev[q++], st);
+      ctx->launches += 1;
+      if (J->pl.probe_bytes) launch_probe<T, EXACT>(ctx, J, s, par, st);  // untimed
+      continue;
+    }
     if (J->d.mode == OIDT_MODE_YEE3D) {
       const bool vec = J->pl.variant == kVariantVec;
       cudaEventRecord(ev[q++], st);
@@ -1265,6 +1357,8 @@ int32_t oidt_job_create(oidt_ctx *ctx, const oidt_job_desc *desc, uint64_t *job)
   }
   // Host pointers are not kept.
   memset(J->d.cb, 0, sizeof J->d.cb);
+  J->d.mat_idx = nullptr;
+  J->d.mat_tab = nullptr;
   memset(J->d.kdx, 0, sizeof J->d.kdx);
   J->d.be = J->d.ce = J->d.bh = J->d.ch = J->d.j_src = nullptr;
   J->d.cos_e = J->d.sin_e = J->d.cos_h = J->d.sin_h = nullptr;
@@ -1330,7 +1424,9 @@ int32_t oidt_job_sync(oidt_ctx *ctx, uint64_t job, int32_t timeout_ms) {
     if (J && J->done == ev) J->busy = cudaEventQuery(ev) != cudaSuccess;
     int flags[2] = {0, 0};
     if (cudaMemcpy(flags, state, sizeof flags, cudaMemcpyDeviceToHost) == cudaSuccess && flags[1])
-      return fail(ctx, OIDT_ERR_TIMEOUT, "a kernel's bounded wait on its tile loads expired (device flag %d)", flags[1]);
+      return fail(ctx, OIDT_ERR_TIMEOUT,
+                  "a kernel's bounded wait expired (device flag %d: 1 = the plane sweep's tile loads, "
+                  "2 = the ordered form's plane order)", flags[1]);
   }
   return rc;
 }
@@ -1678,6 +1774,8 @@ int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_acc, 0, pl.off_state - pl.off_acc, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_state, 0, 64, st));
   if (pl.probe_bytes) CU(ctx, cudaMemsetAsync(J->mem + pl.off_probe, 0, pl.probe_bytes, st));
+  if (pl.variant == kVariantWave)  // the ordered form's counters restart with the steps
+    CU(ctx, cudaMemsetAsync(J->mem + pl.off_wave, 0, 8 + (size_t)4 * (J->d.ie - J->d.ib), st));
   CU(ctx, cudaEventRecord(J->done, st));
   J->busy = true;
   J->steps_enqueued = 0;

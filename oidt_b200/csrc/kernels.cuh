@@ -61,6 +61,15 @@ template <> struct Ar<double, false> {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Bound on every in-kernel wait for other blocks' or copies' progress.
+constexpr long long kWaitCycles = 4000000000LL;  // about 2 s at 1.9 GHz
+
+__device__ __forceinline__ int ld_acquire(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 // ---------------------------------------------------------------------------
 // Job parameters (device-resident copy for batched launches).
 // ---------------------------------------------------------------------------
@@ -72,6 +81,8 @@ template <typename T> struct Params {
   T *f[6];               // fields (read; updated in place by the per-cell launches)
   T *fn[6];              // fields written by the plane sweep (the other buffer)
   const T *cb[3];        // dt/eps per E component (TM2 uses cb[2] for Ez)
+  const unsigned char *mat;  // 3D material index [nx][ny][nzp] (nullptr: none) ...
+  const T *mtab;             // ... and its table [256][4] (CBX, CBY, CBZ, 0)
   const T *kd[6];        // kappa*dx: kxe kye kze kxh kyh kzh
   const T *rkd[6];       // reciprocals
   const T *be, *ce, *bh, *ch;
@@ -143,11 +154,18 @@ __device__ __forceinline__ void capture(const Params<T> &p, int s, int port, int
 //   e(f, di, dj, dk)   new E component f at (i+di, j+dj, k+dk), offsets in {-1,0}
 //   eold(f), hold(f), cb(a)
 // ---------------------------------------------------------------------------
-template <typename T> struct GlobalAcc3 {
+// Loads of E in an H update: L2 only (CG) where the same launch may have
+// written E on another SM (an SM's L1 is not kept coherent with those writes),
+// the read-only path otherwise.
+template <bool CG, typename T> __device__ __forceinline__ T ld_e(const T *q) { return CG ? __ldcg(q) : __ldg(q); }
+
+template <typename T, bool CG = false> struct GlobalAcc3 {
   const Params<T> &p;
   long long c, sy, sx;
   __device__ __forceinline__ T h(int f, int di, int dj, int dk) const { return p.f[f][c + di * sx + dj * sy + dk]; }
-  __device__ __forceinline__ T e(int f, int di, int dj, int dk) const { return p.f[f][c + di * sx + dj * sy + dk]; }
+  __device__ __forceinline__ T e(int f, int di, int dj, int dk) const {
+    return CG ? __ldcg(p.f[f] + (c + di * sx + dj * sy + dk)) : p.f[f][c + di * sx + dj * sy + dk];
+  }
   __device__ __forceinline__ T eold(int f) const { return p.f[f][c]; }
   __device__ __forceinline__ T hold(int f) const { return p.f[f][c]; }
   __device__ __forceinline__ T cb(int a) const { return p.cb[a][c]; }
@@ -367,11 +385,11 @@ __device__ __forceinline__ void y3_e_cell(const Params<T> &p, int i, int j, int 
   y3_capture_e(p, s, i, j, k, m, e);
 }
 
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, bool CG = false>
 __device__ __forceinline__ void y3_h_cell(const Params<T> &p, int i, int j, int k, int n, int s) {
   const long long sy = p.nzp, sx = (long long)p.ny * p.nzp;
   const long long c = i * sx + j * sy + k;
-  GlobalAcc3<T> a{p, c, sy, sx};
+  GlobalAcc3<T, CG> a{p, c, sy, sx};
   T h[3];
   const int m = y3_h_compute<T, EXACT>(p, a, i, j, k, n, h);
   if (m & 1) p.f[HX][c] = h[0];
@@ -470,7 +488,7 @@ __device__ __forceinline__ void y3_e_masked(const Params<T> &p, int i, int j, in
 
 // H update of one cell (i, j, k) away from the source box (as y3_h_compute;
 // ib, jb >= 1, so every neighbour read stays inside the grid arrays).
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, bool CG = false>
 __device__ __forceinline__ void y3_h_masked(const Params<T> &p, int i, int j, int k, int s) {
   const int P = p.P;
   // nothing is updated outside [ib, ie) x [jb, je); inside, every neighbour
@@ -485,11 +503,11 @@ __device__ __forceinline__ void y3_h_masked(const Params<T> &p, int i, int j, in
   // Hz i (ib,ie) j (jb,je) k [kb,ke)
   const bool ko = k > p.kb && k < p.ke, kc = k >= p.kb && k < p.ke;
   const bool mhx = j > p.jb && ko, mhy = i > p.ib && ko, mhz = i > p.ib && j > p.jb && kc;
-  const T ex0 = __ldg(ex + o), ey0 = __ldg(ey + o), ez0 = __ldg(ez + o);
+  const T ex0 = ld_e<CG>(ex + o), ey0 = ld_e<CG>(ey + o), ez0 = ld_e<CG>(ez + o);
   // (k - 1 is read only where k > kb >= 1)
-  const T dey_z = A::sub(ey0, ko ? __ldg(ey + (o - 1)) : ey0), dez_y = A::sub(ez0, __ldg(ez + (o - sy)));
-  const T dez_x = A::sub(ez0, __ldg(ez - sx + o)), dex_z = A::sub(ex0, ko ? __ldg(ex + (o - 1)) : ex0);
-  const T dex_y = A::sub(ex0, __ldg(ex + (o - sy))), dey_x = A::sub(ey0, __ldg(ey - sx + o));
+  const T dey_z = A::sub(ey0, ko ? ld_e<CG>(ey + (o - 1)) : ey0), dez_y = A::sub(ez0, ld_e<CG>(ez + (o - sy)));
+  const T dez_x = A::sub(ez0, ld_e<CG>(ez - sx + o)), dex_z = A::sub(ex0, ko ? ld_e<CG>(ex + (o - 1)) : ex0);
+  const T dex_y = A::sub(ex0, ld_e<CG>(ex + (o - sy))), dey_x = A::sub(ey0, ld_e<CG>(ey - sx + o));
   const T rkx = p.rkd[3][i], rky = p.rkd[4][j], rkz = p.rkd[5][k];
   const T kx = EXACT ? p.kd[3][i] : T(0), ky = EXACT ? p.kd[4][j] : T(0), kz = EXACT ? p.kd[5][k] : T(0);
   const T db = p.db;

@@ -58,7 +58,6 @@ struct SweepItem {
 // E-box of the CTA: TBY x TBZ threads, owned tile (TBY-1) x (TBZ-1).
 constexpr int kSweepEY = 8, kSweepEZ = 32, kSweepStages = 3;
 constexpr int kSweepTY = kSweepEY - 1, kSweepTZ = kSweepEZ - 1;  // owned tile
-constexpr long long kWaitCycles = 4000000000LL;                  // ~2 s at 1.9 GHz
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -74,6 +73,17 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
   unsigned ok;
   asm volatile(
       "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Non-blocking probe (mbarrier.try_wait may suspend the thread until the
+// phase completes; a short bound needs probes that return at once).
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity)
       : "memory");
@@ -190,13 +200,16 @@ __global__ void __launch_bounds__(TBY *TBZ, sizeof(T) == 4 ? 4 : 2)
     for (int a = 0; a < 3; ++a) tma_load_3d(dst + (6 + a) * BOXS, tmc + a * 128, zb, y0 - 1, xi, b);
   };
   // plane u lives in stage u % S and completes that stage's phase u / S
+  // try_wait may suspend the thread until the phase completes, so below the
+  // default bound the probes are non-blocking and the clock is read between them
   auto wait_for = [&](int k, unsigned parity, long long limit) -> bool {
-    if (mbar_try_wait(bar + k, parity)) return true;
+    if (mbar_test_wait(bar + k, parity)) return true;
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar + k, parity)) {
+    const bool suspend = limit >= kWaitCycles;
+    for (;;) {
+      if (suspend ? mbar_try_wait(bar + k, parity) : mbar_test_wait(bar + k, parity)) return true;
       if (clock64() - t0 > limit) return false;
     }
-    return true;
   };
   auto wait = [&](int k, unsigned parity) -> bool { return wait_for(k, parity, p.wait_cycles); };
 

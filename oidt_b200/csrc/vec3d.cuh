@@ -34,11 +34,13 @@
 namespace oidt {
 
 constexpr int kVecThreads = 128;
-// Six resident blocks per SM (at most 80 registers a thread): the vector
-// role's loads in flight come from occupancy, and the edge role's longer code
-// would otherwise raise the whole kernel's register count (measured: with six
-// blocks C2 73.9 us and a 384 x 384 x 256 grid 0.612 ms per step, against 83.6
-// and 0.694 with the compiler's own 96-107 registers).
+// Six resident blocks per SM in FP32 (at most 80 registers a thread): the
+// vector role's loads in flight come from occupancy, and the edge role's
+// longer code would otherwise raise the whole kernel's register count
+// (measured: with six blocks C2 73.9 us and a 384 x 384 x 256 grid 0.612 ms
+// per step, against 83.6 and 0.694 with the compiler's own 96-107 registers).
+// FP64 values take two registers each: three blocks (170 registers) keep the
+// FP64 kernels from spilling.
 constexpr int kVecBlocksPerSM = 6;
 
 template <typename T> struct V4 { T v[4]; };
@@ -50,6 +52,18 @@ __device__ __forceinline__ void ld4(V4<float> &a, const float *p) {
 }
 __device__ __forceinline__ void ld4(V4<double> &a, const double *p) {
   const double2 x = __ldg(reinterpret_cast<const double2 *>(p)), y = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+  a.v[0] = x.x; a.v[1] = x.y; a.v[2] = y.x; a.v[3] = y.y;
+}
+// E in an H update: L2 only (CG) where the same launch may have written E on
+// another SM, whose writes an SM's L1 does not see; the read-only path otherwise
+template <bool CG> __device__ __forceinline__ void ld4e(V4<float> &a, const float *p) {
+  if (!CG) return ld4(a, p);
+  const float4 x = __ldcg(reinterpret_cast<const float4 *>(p));
+  a.v[0] = x.x; a.v[1] = x.y; a.v[2] = x.z; a.v[3] = x.w;
+}
+template <bool CG> __device__ __forceinline__ void ld4e(V4<double> &a, const double *p) {
+  if (!CG) return ld4(a, p);
+  const double2 x = __ldcg(reinterpret_cast<const double2 *>(p)), y = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
   a.v[0] = x.x; a.v[1] = x.y; a.v[2] = y.x; a.v[3] = y.y;
 }
 // data this launch also writes (each element only by the thread reading it)
@@ -67,6 +81,31 @@ __device__ __forceinline__ void st4(float *p, const float (&v)[4]) {
 __device__ __forceinline__ void st4(double *p, const double (&v)[4]) {
   reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
   reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+
+// dt/eps of four cells: from the material index and its table (one byte per
+// cell, the table entries read through L1) or from the three grids.
+__device__ __forceinline__ void tab_entry(const float *t, unsigned q, float &a, float &b, float &c) {
+  const float4 e = __ldg(reinterpret_cast<const float4 *>(t) + q);
+  a = e.x; b = e.y; c = e.z;
+}
+__device__ __forceinline__ void tab_entry(const double *t, unsigned q, double &a, double &b, double &c) {
+  const double2 e = __ldg(reinterpret_cast<const double2 *>(t) + 2 * q), f = __ldg(reinterpret_cast<const double2 *>(t) + 2 * q + 1);
+  a = e.x; b = e.y; c = f.x;
+}
+template <typename T>
+__device__ __forceinline__ void load_cb(const Params<T> &p, long long bi, int o, V4<T> &C0, V4<T> &C1, V4<T> &C2) {
+  if (p.mat) {
+    const uchar4 m = __ldg(reinterpret_cast<const uchar4 *>(p.mat + bi + o));
+    tab_entry(p.mtab, m.x, C0.v[0], C1.v[0], C2.v[0]);
+    tab_entry(p.mtab, m.y, C0.v[1], C1.v[1], C2.v[1]);
+    tab_entry(p.mtab, m.z, C0.v[2], C1.v[2], C2.v[2]);
+    tab_entry(p.mtab, m.w, C0.v[3], C1.v[3], C2.v[3]);
+  } else {
+    ld4(C0, p.cb[0] + bi + o);
+    ld4(C1, p.cb[1] + bi + o);
+    ld4(C2, p.cb[2] + bi + o);
+  }
 }
 
 // Split of a row between the roles (computed on the host per job).
@@ -89,9 +128,10 @@ template <typename T> __device__ __forceinline__ bool near_src(const Params<T> &
 // tested per cell and the z-slab psi read and written per cell (all old
 // values of a group read before the first write).  Groups within one cell of
 // the source box run y3_e_cell / y3_h_cell per cell.
-template <typename T> __device__ __forceinline__ bool edge_group(const Params<T> &p, const VecGeom &g, int &j, int &k0) {
+template <typename T>
+__device__ __forceinline__ bool edge_group(const Params<T> &p, const VecGeom &g, int bx, int &j, int &k0) {
   const int nge = g.nedge >> 2;
-  const int t = (blockIdx.x - g.nb_vec) * kVecThreads + threadIdx.x;
+  const int t = (bx - g.nb_vec) * kVecThreads + threadIdx.x;
   if (t >= (p.je - p.jb) * nge) return false;
   const int r = t / nge, e4 = 4 * (t - r * nge);
   j = p.jb + r;
@@ -100,9 +140,9 @@ template <typename T> __device__ __forceinline__ bool edge_group(const Params<T>
 }
 
 template <typename T, bool EXACT>
-__device__ __forceinline__ void v3_edge_e(const Params<T> &p, const VecGeom &g, int i, int s) {
+__device__ __forceinline__ void v3_edge_e(const Params<T> &p, const VecGeom &g, int i, int bx, int s) {
   int j, k0;
-  if (!edge_group(p, g, j, k0)) return;
+  if (!edge_group(p, g, bx, j, k0)) return;
   if (near_src(p, i, j, k0, 4)) {
     for (int m = 0; m < 4; ++m)
       if (k0 + m < p.nz) y3_e_cell<T, EXACT>(p, i, j, k0 + m, p.state[0] + s, s);
@@ -134,9 +174,7 @@ __device__ __forceinline__ void v3_edge_e(const Params<T> &p, const VecGeom &g, 
   ld4(Hyx, hy + sx + o);
   const bool kn = k0 + 4 < p.nzp;  // the k + 1 neighbour of the last cell
   const T hyk = kn ? __ldg(hy + (o + 4)) : T(0), hxk = kn ? __ldg(hx + (o + 4)) : T(0);
-  ld4(C0, p.cb[0] + bi + o);
-  ld4(C1, p.cb[1] + bi + o);
-  ld4(C2, p.cb[2] + bi + o);
+  load_cb(p, bi, o, C0, C1, C2);
   T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
   ldw4(Ex, ex + o);
   ldw4(Ey, ey + o);
@@ -255,13 +293,13 @@ __device__ __forceinline__ void v3_edge_e(const Params<T> &p, const VecGeom &g, 
   }
 }
 
-template <typename T, bool EXACT>
-__device__ __forceinline__ void v3_edge_h(const Params<T> &p, const VecGeom &g, int i, int s) {
+template <typename T, bool EXACT, bool CG>
+__device__ __forceinline__ void v3_edge_h(const Params<T> &p, const VecGeom &g, int i, int bx, int s) {
   int j, k0;
-  if (!edge_group(p, g, j, k0)) return;
+  if (!edge_group(p, g, bx, j, k0)) return;
   if (near_src(p, i, j, k0, 4)) {
     for (int m = 0; m < 4; ++m)
-      if (k0 + m < p.nz) y3_h_cell<T, EXACT>(p, i, j, k0 + m, p.state[0] + s, s);
+      if (k0 + m < p.nz) y3_h_cell<T, EXACT, CG>(p, i, j, k0 + m, p.state[0] + s, s);
     return;
   }
   using A = Ar<T, EXACT>;
@@ -281,15 +319,15 @@ __device__ __forceinline__ void v3_edge_h(const Params<T> &p, const VecGeom &g, 
   const int o = j * sy + k0;
   const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
   V4<T> Ex, Ey, Ez, Ezy, Exy, Ezx, Eyx, Hx, Hy, Hz, Rz, Kz;
-  ld4(Ex, ex + o);
-  ld4(Ey, ey + o);
-  ld4(Ez, ez + o);
-  ld4(Ezy, ez + (o - sy));
-  ld4(Exy, ex + (o - sy));
-  ld4(Ezx, ez - sx + o);
-  ld4(Eyx, ey - sx + o);
+  ld4e<CG>(Ex, ex + o);
+  ld4e<CG>(Ey, ey + o);
+  ld4e<CG>(Ez, ez + o);
+  ld4e<CG>(Ezy, ez + (o - sy));
+  ld4e<CG>(Exy, ex + (o - sy));
+  ld4e<CG>(Ezx, ez - sx + o);
+  ld4e<CG>(Eyx, ey - sx + o);
   const bool kp = k0 > 0;  // the k - 1 neighbour of the first cell
-  const T eyk = kp ? __ldg(ey + (o - 1)) : T(0), exk = kp ? __ldg(ex + (o - 1)) : T(0);
+  const T eyk = kp ? ld_e<CG>(ey + (o - 1)) : T(0), exk = kp ? ld_e<CG>(ex + (o - 1)) : T(0);
   T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
   ldw4(Hx, hx + o);
   ldw4(Hy, hy + o);
@@ -418,15 +456,14 @@ __device__ __forceinline__ void v3_edge_h(const Params<T> &p, const VecGeom &g, 
 // j (jb,je) k [kb,ke); Ez i [ib,ie) j [jb,je) k (kb,ke).  Grid: (vector-role
 // then edge-role blocks, x-planes ib..ie-1).
 // ---------------------------------------------------------------------------
+// One block of x-plane i: bx < nb_vec a vector-role block, the edge role above.
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_e(Params<T> p, VecGeom g, int s) {
-  pdl_wait();
-  const int i = p.ib + blockIdx.y;
-  if ((int)blockIdx.x >= g.nb_vec) {
-    v3_edge_e<T, EXACT>(p, g, i, s);
+__device__ __forceinline__ void v3_e_block(const Params<T> &p, const VecGeom &g, int i, int bx, int s) {
+  if (bx >= g.nb_vec) {
+    v3_edge_e<T, EXACT>(p, g, i, bx, s);
     return;
   }
-  const int t = blockIdx.x * kVecThreads + threadIdx.x;
+  const int t = bx * kVecThreads + threadIdx.x;
   if (t >= (p.je - p.jb) * g.nvc) return;
   const int r = t / g.nvc;
   const int j = p.jb + r, k0 = g.kz0 + 4 * (t - r * g.nvc);
@@ -448,9 +485,7 @@ __global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_e(Params<T>
   ld4(Hzx, hz + sx + o);
   ld4(Hyx, hy + sx + o);
   const T hyk = __ldg(hy + (o + 4)), hxk = __ldg(hx + (o + 4));  // k0 + 4 < kz1 <= nz - 2
-  ld4(C0, p.cb[0] + bi + o);
-  ld4(C1, p.cb[1] + bi + o);
-  ld4(C2, p.cb[2] + bi + o);
+  load_cb(p, bi, o, C0, C1, C2);
   T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
   ldw4(Ex, ex + o);
   ldw4(Ey, ey + o);
@@ -560,15 +595,13 @@ __global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_e(Params<T>
 // decreasing i: the launch starts on the E planes the E half-step wrote last
 // (still in L2) and ends on the planes the next E half-step reads first.
 // ---------------------------------------------------------------------------
-template <typename T, bool EXACT>
-__global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_h(Params<T> p, VecGeom g, int s) {
-  pdl_wait();
-  const int i = p.ie - 1 - blockIdx.y;
-  if ((int)blockIdx.x >= g.nb_vec) {
-    v3_edge_h<T, EXACT>(p, g, i, s);
+template <typename T, bool EXACT, bool CG>
+__device__ __forceinline__ void v3_h_block(const Params<T> &p, const VecGeom &g, int i, int bx, int s) {
+  if (bx >= g.nb_vec) {
+    v3_edge_h<T, EXACT, CG>(p, g, i, bx, s);
     return;
   }
-  const int t = blockIdx.x * kVecThreads + threadIdx.x;
+  const int t = bx * kVecThreads + threadIdx.x;
   if (t >= (p.je - p.jb) * g.nvc) return;
   const int r = t / g.nvc;
   const int j = p.jb + r, k0 = g.kz0 + 4 * (t - r * g.nvc);
@@ -578,14 +611,14 @@ __global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_h(Params<T>
   const int o = j * sy + k0;
   const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
   V4<T> Ex, Ey, Ez, Ezy, Exy, Ezx, Eyx, Hx, Hy, Hz, Rz, Kz;
-  ld4(Ex, ex + o);
-  ld4(Ey, ey + o);
-  ld4(Ez, ez + o);
-  ld4(Ezy, ez + (o - sy));
-  ld4(Exy, ex + (o - sy));
-  ld4(Ezx, ez - sx + o);
-  ld4(Eyx, ey - sx + o);
-  const T eyk = __ldg(ey + (o - 1)), exk = __ldg(ex + (o - 1));  // k0 - 1 >= kz0 - 1 >= kb + P - 1
+  ld4e<CG>(Ex, ex + o);
+  ld4e<CG>(Ey, ey + o);
+  ld4e<CG>(Ez, ez + o);
+  ld4e<CG>(Ezy, ez + (o - sy));
+  ld4e<CG>(Exy, ex + (o - sy));
+  ld4e<CG>(Ezx, ez - sx + o);
+  ld4e<CG>(Eyx, ey - sx + o);
+  const T eyk = ld_e<CG>(ey + (o - 1)), exk = ld_e<CG>(ex + (o - 1));  // k0 - 1 >= kz0 - 1 >= kb + P - 1
   T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
   ldw4(Hx, hx + o);
   ldw4(Hy, hy + o);
@@ -691,6 +724,82 @@ __global__ void __launch_bounds__(kVecThreads, kVecBlocksPerSM) k_v3_h(Params<T>
       }
     }
   }
+}
+
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSM : 3) k_v3_e(Params<T> p, VecGeom g, int s) {
+  pdl_wait();
+  v3_e_block<T, EXACT>(p, g, p.ib + blockIdx.y, blockIdx.x, s);
+}
+
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSM : 3) k_v3_h(Params<T> p, VecGeom g, int s) {
+  pdl_wait();
+  v3_h_block<T, EXACT, false>(p, g, p.ie - 1 - blockIdx.y, blockIdx.x, s);
+}
+
+// ---------------------------------------------------------------------------
+// Ordered form: one launch per time step runs both half-steps, plane by
+// plane, in the order E(0), E(1), H(0), E(2), H(1), ..., E(n-1), H(n-2),
+// H(n-1) (n = ie - ib updated planes, q = i - ib).  H(q) reads new E of
+// planes q and q-1, and overwrites the H of plane q that E(q) and E(q-1)
+// read, so its blocks wait until every block of E(q) and E(q-1) has finished;
+// no other dependence exists inside a step.  A block takes its place in the
+// order from a ticket (an atomic counter), not from blockIdx, so every block
+// it may wait for has been given an earlier ticket, is resident or done, and
+// waits for nothing itself: the waits end.  Each wait is bounded all the same
+// (kWaitCycles); on expiry the block records state[1] = 2 and returns without
+// updating, and oidt_job_sync reports the job as timed out.  H blocks read E
+// through L2 (another SM's L1 may hold lines written in this launch).  The
+// new E of planes q and q-1 and the H of plane q were touched a few planes
+// earlier, so H reads them from L2, and DRAM carries each field word once
+// per step.
+// ---------------------------------------------------------------------------
+struct WaveArgs {
+  unsigned long long *ticket;  // tickets taken so far (all steps)
+  int *done;                   // [n]: E blocks finished per plane (all steps)
+  int nb;                      // blocks per plane and half-step (vector + edge role)
+};
+
+template <typename T, bool EXACT>
+__global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSM : 3)
+    k_v3_wave(Params<T> p, VecGeom g, WaveArgs w, int s) {
+  pdl_wait();
+  __shared__ long long s_ticket;
+  __shared__ int s_ok;
+  const int n = p.ie - p.ib;
+  const long long step = (long long)p.state[0] + s;             // steps run before this one
+  const long long per_step = 2LL * n * w.nb;
+  if (threadIdx.x == 0) {
+    s_ticket = (long long)atomicAdd(w.ticket, 1ULL) - step * per_step;
+    s_ok = 1;
+  }
+  __syncthreads();
+  const long long t = s_ticket;
+  const int u = (int)(t / w.nb), bx = (int)(t - (long long)u * w.nb);
+  // unit u: 0 -> E(0); odd u < 2n - 1 -> E((u + 1) / 2); even u >= 2 -> H(u / 2 - 1); 2n - 1 -> H(n - 1)
+  const bool is_h = u == 2 * n - 1 || (u >= 2 && (u & 1) == 0);
+  const int q = u == 0 ? 0 : u == 2 * n - 1 ? n - 1 : (u & 1) ? (u + 1) / 2 : u / 2 - 1;
+  if (!is_h) {
+    v3_e_block<T, EXACT>(p, g, p.ib + q, bx, s);
+    __threadfence();  // this thread's stores visible to the whole GPU ...
+    __syncthreads();  // ... for every thread of the block, before the count
+    if (threadIdx.x == 0) atomicAdd(w.done + q, 1);
+    return;
+  }
+  if (threadIdx.x == 0) {
+    const int want = (int)((step + 1) * w.nb);
+    const long long t0 = clock64();
+    for (int d = 0; d < 2 && q - d >= 0 && s_ok; ++d)
+      while (ld_acquire(w.done + (q - d)) < want)
+        if (clock64() - t0 > kWaitCycles) {
+          atomicExch(p.state + 1, 2);  // reported to the host by oidt_job_sync
+          s_ok = 0;
+          break;
+        }
+  }
+  __syncthreads();
+  if (s_ok) v3_h_block<T, EXACT, true>(p, g, p.ib + q, bx, s);
 }
 
 }  // namespace oidt

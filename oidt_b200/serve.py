@@ -290,15 +290,16 @@ def accuracy_sample(eng: Engine, requests, results, per_kind: int = 4, seed: int
         pool = [r for r in results if r.kind == kind]
         for r in rng.choice(pool, size=min(per_kind, len(pool)), replace=False):
             q = by_rid[r.rid]
-            j = eng.submit(q.spec, arith="exact", precision=np.float64)
-            ji = eng.submit(q.incident, arith="exact", precision=np.float64) if q.incident is not None else None
+            spec, inc = q.build() if q.build is not None else (q.spec, q.incident)  # served specs dropped their arrays
+            j = eng.submit(spec, arith="exact", precision=np.float64)
+            ji = eng.submit(inc, arith="exact", precision=np.float64) if inc is not None else None
             j.run()
             if ji is not None:
                 ji.run()
             j.sync()
             if ji is not None:
                 ji.sync()
-            S = forward_s_device(q.spec, ji if ji is not None else j, j)
+            S = forward_s_device(spec, ji if ji is not None else j, j)
             for x in (j, ji):
                 if x is not None:
                     x.release()

@@ -51,6 +51,10 @@ class SimSpec:
     twiddles: tuple   # cosE, sinE, cosH, sinH, float64 [nf][nt]
     nt: int
     meta: dict = field(default_factory=dict)
+    # optional (3D): the dt/eps grids as a one-byte material index [nx][ny][nz]
+    # and its float64 table [nmat][3]; tab[idx] equals (cb['x'], cb['y'], cb['z'])
+    mat_idx: np.ndarray = None
+    mat_tab: np.ndarray = None
 
     @property
     def ncells(self) -> int:
@@ -81,10 +85,11 @@ class JobDesc(C.Structure):
         ("port_pos", C.c_int32 * 2), ("win_lo", C.c_int32 * 2), ("win_hi", C.c_int32 * 2),
         ("cos_e", C.c_void_p), ("sin_e", C.c_void_p), ("cos_h", C.c_void_p), ("sin_h", C.c_void_p),
         ("ring_steps", C.c_int32), ("reserved", C.c_int32 * 4), ("probe", C.c_int32 * 3),
+        ("mat_idx", C.c_void_p), ("mat_tab", C.c_void_p), ("nmat", C.c_int32),
     ]
 
 
-VARIANTS = {"cell": 0, "sweep": 1, "vec": 2}
+VARIANTS = {"cell": 0, "sweep": 1, "vec": 2, "wave": 3}
 
 
 def power_window(spec: SimSpec):
@@ -98,18 +103,21 @@ def power_window(spec: SimSpec):
 
 
 def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "vec",
-            graphs: bool = True, rows: int = 0, march_depth: int = 0):
+            graphs: bool = True, rows: int = 0, march_depth: int = 0, material: bool = True):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
     ``keepalive`` must outlive the ``oidt_job_create`` call.
 
     ``variant`` (3D only): 'vec' (default) -- the E-half / H-half launches
-    with four cells per thread along z and 16-byte accesses; 'cell' -- the
-    same half-steps with one cell per thread; 'sweep' -- one plane-sweep
-    launch per step (E and H fused, TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
+    with four cells per thread along z and 16-byte accesses; 'wave' -- the
+    same code in one launch per step, E and H half-steps ordered plane by
+    plane; 'cell' -- the half-steps with one cell per thread; 'sweep' -- one
+    plane-sweep launch per step (E and H fused, TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
     launches every step directly instead of replaying K-step CUDA graphs.
     ``rows`` (3D per-cell form): tile rows of a block, 2, 4 or 8 (0 = 4);
     ``march_depth`` (3D plane sweep): x-planes per work item (0 = the
-    engine's makespan estimate).  ``oidt_b200.tune`` measures both."""
+    engine's makespan estimate).  ``oidt_b200.tune`` measures both.
+    ``material``: pass the spec's material index (if it has one) instead of
+    the three dt/eps grids -- the same values, one byte per cell."""
     prec = np.dtype(precision if precision is not None else spec.precision)
     if prec not in (np.dtype(np.float32), np.dtype(np.float64)):
         raise ValueError("precision must be float32 or float64")
@@ -133,9 +141,14 @@ def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int 
     d.ie, d.je, d.ke = hi
     d.nt = spec.nt
     d.nf = spec.nf
-    for slot, ax in enumerate("xyz"):
-        if ax in spec.cb:
-            d.cb[slot] = arr(spec.cb[ax])
+    if material and spec.mat_idx is not None and spec.mode == "yee3d":
+        d.mat_idx = arr(spec.mat_idx, np.uint8)
+        d.mat_tab = arr(spec.mat_tab)
+        d.nmat = len(spec.mat_tab)
+    else:
+        for slot, ax in enumerate("xyz"):
+            if ax in spec.cb:
+                d.cb[slot] = arr(spec.cb[ax])
     for slot, key in enumerate(("xe", "ye", "ze", "xh", "yh", "zh")):
         if key in spec.kdx:
             d.kdx[slot] = arr(spec.kdx[key])

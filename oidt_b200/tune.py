@@ -37,6 +37,7 @@ from .spec import SimSpec
 
 DEFAULT = {"variant": "vec", "rows": 0, "march_depth": 0}
 CANDIDATES = (
+    {"variant": "wave", "rows": 0, "march_depth": 0},
     {"variant": "vec", "rows": 0, "march_depth": 0},
     {"variant": "cell", "rows": 4, "march_depth": 0},
     {"variant": "cell", "rows": 2, "march_depth": 0},
@@ -47,9 +48,9 @@ CANDIDATES = (
 
 
 def label(choice: dict) -> str:
-    """'vec', 'cell/rows4', 'sweep/depth16', 'sweep/depth-auto'."""
-    if choice["variant"] == "vec":
-        return "vec"
+    """'vec', 'wave', 'cell/rows4', 'sweep/depth16', 'sweep/depth-auto'."""
+    if choice["variant"] in ("vec", "wave"):
+        return choice["variant"]
     if choice["variant"] == "cell":
         return "cell/rows%d" % (choice["rows"] or 4)
     return "sweep/depth%s" % (choice["march_depth"] or "-auto")

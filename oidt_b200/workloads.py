@@ -158,6 +158,8 @@ def strip3d(nx=128, ny=128, nz=256, dx=20e-9, P=10, n_core=3.48, n_clad=1.44, co
     prec = np.float64
     ex, ey, ez = staggered_eps(eps_cell, prec, (0, 1, 2))
     cb = {"x": dt / ex, "y": dt / ey, "z": dt / ez}
+    two = np.array([False, True])
+    mat_idx, mat_tab = material_index(mask, eps * ((n_core ** 2 / eps_bg) * two + 1 * ~two), dt)
     tab = cpml_profiles(P, dx, dt, eps, eta, prec, m_grade=m_grade, kappa_max=kappa_max, alpha_max=alpha_max)
     kdx = {}
     for n, name in ((nx, "x"), (ny, "y"), (nz, "z")):
@@ -175,7 +177,41 @@ def strip3d(nx=128, ny=128, nz=256, dx=20e-9, P=10, n_core=3.48, n_clad=1.44, co
         j_src=wave_packet(steps, dt, C0 / (lam0 * 1e-9), bw), port_pos=(p1, p2),
         win_lo=(P, P), win_hi=(nx - P, ny - P), freqs=freqs, twiddles=twiddles(freqs, dt, steps), nt=steps,
         meta=dict(workload="rib3d" if cs else "strip3d", dt=dt, seed=seed, sigma_nm=sigma_nm, lc_nm=lc_nm,
-                  rough=rough, power_window=((P, nx - P), (P, ny - P)), core=(bx, by, cx, cy), slab_cells=cs))
+                  rough=rough, power_window=((P, nx - P), (P, ny - P)), core=(bx, by, cx, cy), slab_cells=cs),
+        mat_idx=mat_idx, mat_tab=mat_tab)
+
+
+def material_index(mask: np.ndarray, eps_vals: np.ndarray, dt: float):
+    """The dt/eps grids of a two-material 3D grid as a one-byte index and a
+    table, equal to ``dt / staggered_eps(eps_cell)`` cell by cell.
+
+    Every component's permittivity is a 2-point average of the cell and its
+    lower neighbour along the component's axis on cells with all indices >= 1,
+    the cell's own value on the first layer (``refsetup.staggered_eps``).  So
+    a cell's (CBX, CBY, CBZ) depends only on the material of the cell and of
+    its three lower neighbours, or on the cell alone on the first layer: at
+    most 18 codes.  ``eps_vals`` = (cladding, core) permittivity as the
+    permittivity grid holds them; the table entries repeat the grid's float64
+    operations, so they equal the grids' values bit for bit.  Returns
+    (idx uint8 [nx][ny][nz], tab float64 [nmat][3])."""
+    m = mask.astype(np.uint8)
+    code = (17 + m).astype(np.uint8)  # first layer: the cell's own material
+    inner = (slice(1, None),) * 3
+    code[inner] = 1 + m[1:, 1:, 1:] + 2 * m[:-1, 1:, 1:] + 4 * m[1:, :-1, 1:] + 8 * m[1:, 1:, :-1]
+    present = np.nonzero(np.bincount(code.ravel(), minlength=19))[0]
+    lut = np.zeros(19, dtype=np.uint8)
+    lut[present] = np.arange(len(present), dtype=np.uint8)
+    E = np.asarray(eps_vals, dtype=np.float64)
+    tab = np.empty((len(present), 3))
+    for q, c in enumerate(present):
+        if c >= 17:
+            e = np.full(3, E[c - 17])
+        else:
+            b = c - 1
+            own = E[b & 1]
+            e = np.array([0.5 * (own + E[(b >> s) & 1]) for s in (1, 2, 3)])
+        tab[q] = dt / e
+    return lut[code], tab
 
 
 def with_smooth(spec_kwargs: dict) -> dict:

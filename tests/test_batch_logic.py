@@ -58,7 +58,7 @@ class _Engine:
 @pytest.mark.parametrize("ring", [32, 64])
 def test_measure_tunes_first_and_both_legs_use_the_choice(monkeypatch, ring):
     log = []
-    times = {"vec": 0.95, "cell/rows4": 1.0, "cell/rows2": 1.1, "cell/rows8": 0.9, "sweep/depth-auto": 2.0,
+    times = {"wave": 0.96, "vec": 0.95, "cell/rows4": 1.0, "cell/rows2": 1.1, "cell/rows8": 0.9, "sweep/depth-auto": 2.0,
              "sweep/depth16": 2.0}
 
     def fake_time(self, spec, choice, precision=None, arith="fast", ring_steps=32):

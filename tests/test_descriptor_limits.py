@@ -25,8 +25,9 @@ def _bytes(lib, d):
 
 
 def _d3():
+    # the dt/eps grids themselves (the material-index rules: test_material_index.py)
     return to_desc(W.strip3d(nx=20, ny=19, nz=40, P=4, src_gap=2, port_gap=3, steps=30, nf=2, core_x_nm=120,
-                             core_y_nm=160))
+                             core_y_nm=160), material=False)
 
 
 def _d2():
@@ -52,7 +53,7 @@ MUT3 = [
     ("win_lo[1]", -1), ("win_hi[1]", 19), ("win_hi[0]", 20), ("win_lo[0]", 16),
     ("src_field", 6), ("src_lo[2]", 1), ("src_hi[1]", 19),
     ("probe[0]", 2), ("probe[1]", 3),
-    ("reserved[0]", 3), ("reserved[1]", 2), ("reserved[2]", 3), ("reserved[3]", 4),
+    ("reserved[0]", 4), ("reserved[1]", 2), ("reserved[2]", 3), ("reserved[3]", 4),
     ("ring_steps", 4097),
 ]
 

@@ -21,7 +21,7 @@ S_TOL = 1e-4
 CHECKPOINT = 1500
 
 
-@pytest.mark.parametrize("variant", ["cell", "sweep", "vec"])
+@pytest.mark.parametrize("variant", ["cell", "sweep", "vec", "wave"])
 def test_fp32_vs_fp64_exact_at_bench_size(variant):
     eng = Engine(0)
     kw = dict(nx=128, ny=128, nz=256, dx=20e-9, P=10, steps=4000, nf=41, sigma_nm=10.0, lc_nm=50.0, seed=0)

@@ -41,8 +41,9 @@ def _fixture_cases():
 
 
 def _case_variants():
-    """3D runs under every launch form (plane sweep, per-cell, vector); 2D has one."""
-    return [(c, v) for c in _fixture_cases() for v in (("sweep", "cell", "vec") if c.startswith("yee3d") else ("cell",))]
+    """3D runs under every launch form (plane sweep, per-cell, vector, ordered); 2D has one."""
+    return [(c, v) for c in _fixture_cases()
+            for v in (("sweep", "cell", "vec", "wave") if c.startswith("yee3d") else ("cell",))]
 
 
 @pytest.mark.parametrize("case,variant", _case_variants())
@@ -126,12 +127,13 @@ def _te2_spec():
                                   "yee3d_tm_cell", "yee3d_wide_cell", "yee3d_p1", "yee3d_p1_cell",
                                   "yee3d_p2", "yee3d_p2_cell", "tm2_p1", "yee3d_graded", "yee3d_graded_cell",
                                   "yee3d_te_vec", "yee3d_tm_vec", "yee3d_wide_vec", "yee3d_p1_vec", "yee3d_p2_vec",
-                                  "yee3d_graded_vec"])
+                                  "yee3d_graded_vec", "yee3d_te_wave", "yee3d_tm_wave", "yee3d_wide_wave",
+                                  "yee3d_p1_wave", "yee3d_p2_wave", "yee3d_graded_wave"])
 @pytest.mark.parametrize("ring", [1, 7, 32])
 def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     base, _, suffix = name.rpartition("_")
-    variant = {"cell": "cell", "vec": "vec"}.get(suffix, "sweep")
-    base = base if suffix in ("cell", "vec") else name
+    variant = {"cell": "cell", "vec": "vec", "wave": "wave"}.get(suffix, "sweep")
+    base = base if suffix in ("cell", "vec", "wave") else name
     spec = _te2_spec() if base == "te2" else _random_cases()[base]()
     rng = np.random.default_rng(sum(map(ord, name)) + ring)
     s = oracle_from_spec(spec)
@@ -158,7 +160,8 @@ def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
 
 @pytest.mark.parametrize("choice", [{"variant": "cell", "rows": 2}, {"variant": "cell", "rows": 8},
                                     {"variant": "sweep", "march_depth": 1}, {"variant": "sweep", "march_depth": 3},
-                                    {"variant": "sweep", "march_depth": 500}, {"variant": "vec"}])
+                                    {"variant": "sweep", "march_depth": 500}, {"variant": "vec"},
+                                    {"variant": "wave"}])
 @pytest.mark.parametrize("name", ["yee3d_te", "yee3d_tm", "yee3d_wide", "yee3d_graded"])
 def test_launch_choices_equal_oracle(eng, name, choice):
     """Every launch choice the tuner may pick (tile rows 2 and 8 with ragged
@@ -235,7 +238,7 @@ def test_fp32_slab2d_full_run_within_targets(eng):
     job.release()
 
 
-@pytest.mark.parametrize("variant", ["cell", "sweep", "vec"])
+@pytest.mark.parametrize("variant", ["cell", "sweep", "vec", "wave"])
 def test_fp32_strip3d_within_targets(eng, variant):
     """A reduced 3D rough strip (64 x 56 x 120, 700 steps) in float32 vs the
     float64 oracle on identical inputs, both 3D launch forms."""
@@ -265,12 +268,12 @@ def test_fp32_strip3d_within_targets(eng, variant):
 
 def test_batch_equals_single_jobs(eng):
     """One multi-job advance over jobs of different solvers and sizes (2D TM,
-    2D TE, 3D sweep, 3D per-cell, 3D vector form) equals advancing each job
+    2D TE, 3D sweep, 3D per-cell, 3D vector and ordered forms) equals advancing each job
     alone, bit for bit (float64 EXACT), including an odd tail that flips
     sweep buffers."""
     specs = [_random_cases()["tm2"](), _te2_spec(), _random_cases()["yee3d_te"](), _random_cases()["yee3d_tm"](),
-             _random_cases()["yee3d_wide"]()]
-    variants = ["cell", "cell", "sweep", "cell", "vec"]
+             _random_cases()["yee3d_wide"](), _random_cases()["yee3d_p2"]()]
+    variants = ["cell", "cell", "sweep", "cell", "vec", "wave"]
     solo, mix = [], []
     for sp, v in zip(specs, variants):
         solo.append(eng.submit(sp, arith="exact", precision=np.float64, ring_steps=6, variant=v))
