@@ -327,7 +327,7 @@ struct JobPlan {
   size_t off_probe, probe_bytes;  // line probe [4][nt][nx] (probe_bytes = 0: none)
   size_t off_mat, off_mtab;       // material index [nx][ny][nzp] and table [256][4] (3D, optional)
   bool mat;
-  size_t off_wave;                // ordered form: ticket counter (8 B) and E-block counts per plane
+  size_t off_wave;                // ordered form: E-block counts per plane (after 8 spare bytes)
   size_t off_pow;                 // port power [nf] complex float64
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
@@ -895,12 +895,20 @@ template <typename T, bool EXACT> void v3_half(bool H, bool pdl, const Params<T>
 
 // One time step of the ordered form: both half-steps, plane by plane, in one
 // launch of 2 (ie - ib) blocks per plane and half-step (k_v3_wave).
+// The ordered form's lag: as many planes as keep the arrays a plane of the
+// step touches (six fields, the dt/eps grids) within 32 MB of L2, 2 to 32.
+template <typename T> int wave_lag(const Params<T> &p) {
+  const double plane = (double)p.ny * p.nzp * sizeof(T) * 9;
+  const int n = p.ie - p.ib;
+  return std::max(1, std::min(n, std::max(2, std::min(32, (int)(32.0e6 / plane)))));
+}
+
 template <typename T, bool EXACT> void v3_wave(Job *J, bool pdl, const Params<T> &p, int s, cudaStream_t st) {
   const VecGeom g = vec_geom(p);
   WaveArgs w;
-  w.ticket = reinterpret_cast<unsigned long long *>(J->mem + J->pl.off_wave);
   w.done = reinterpret_cast<int *>(J->mem + J->pl.off_wave + 8);
   w.nb = g.nb_vec + vec_edge_blocks(g, p.jb, p.je);
+  w.lag = wave_lag(p);
   const dim3 grd((unsigned)(2LL * (p.ie - p.ib) * w.nb)), blk(kVecThreads);
   if (pdl) launch_step_kernel(k_v3_wave<T, EXACT>, grd, blk, 0, st, p, g, w, s);
   else k_v3_wave<T, EXACT><<<grd, blk, 0, st>>>(p, g, w, s);

@@ -740,46 +740,50 @@ __global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSM 
 
 // ---------------------------------------------------------------------------
 // Ordered form: one launch per time step runs both half-steps, plane by
-// plane, in the order E(0), E(1), H(0), E(2), H(1), ..., E(n-1), H(n-2),
-// H(n-1) (n = ie - ib updated planes, q = i - ib).  H(q) reads new E of
-// planes q and q-1, and overwrites the H of plane q that E(q) and E(q-1)
-// read, so its blocks wait until every block of E(q) and E(q-1) has finished;
-// no other dependence exists inside a step.  A block takes its place in the
-// order from a ticket (an atomic counter), not from blockIdx, so every block
-// it may wait for has been given an earlier ticket, is resident or done, and
-// waits for nothing itself: the waits end.  Each wait is bounded all the same
-// (kWaitCycles); on expiry the block records state[1] = 2 and returns without
-// updating, and oidt_job_sync reports the job as timed out.  H blocks read E
-// through L2 (another SM's L1 may hold lines written in this launch).  The
-// new E of planes q and q-1 and the H of plane q were touched a few planes
-// earlier, so H reads them from L2, and DRAM carries each field word once
-// per step.
+// plane: E(0) .. E(D-1), then for q = 0 .. n-1 the pair E(q+D) (while q+D <
+// n), H(q) -- a unit of nb blocks each, n = ie - ib updated planes, q = i -
+// ib, D the lag (wave.lag).  H(q) reads new E of planes q and q-1 and
+// overwrites the H of plane q that E(q) and E(q-1) read, so its blocks wait
+// until every block of E(q) and E(q-1) has finished; no other dependence
+// exists inside a step.  A block's place in the order is its block index; the
+// hardware dispatches a 1D grid in increasing block index, so the E blocks an
+// H block waits for were dispatched D units or more earlier, and those never
+// wait: the waits end, and with the lag they are rarely needed at all.  Each
+// wait is bounded (kWaitCycles); on expiry the block records state[1] = 2
+// and returns without updating, and oidt_job_sync reports the job as timed
+// out -- should a dependence ever not be resident, the launch ends with that
+// error instead of hanging.  H blocks read E through L2 (another SM's L1 may
+// hold lines written in this launch).  The new E of planes q and q-1 and the
+// H of plane q were touched D units earlier, and D is chosen so that D planes
+// of the step's arrays fit in L2: H reads them from L2 and DRAM carries each
+// field word about once per step.
 // ---------------------------------------------------------------------------
 struct WaveArgs {
-  unsigned long long *ticket;  // tickets taken so far (all steps)
-  int *done;                   // [n]: E blocks finished per plane (all steps)
-  int nb;                      // blocks per plane and half-step (vector + edge role)
+  int *done;  // [n]: E blocks finished per plane, summed over the steps run
+  int nb;     // blocks per plane and half-step (vector + edge role)
+  int lag;    // D, 1 <= D <= n
 };
 
 template <typename T, bool EXACT>
 __global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSM : 3)
     k_v3_wave(Params<T> p, VecGeom g, WaveArgs w, int s) {
   pdl_wait();
-  __shared__ long long s_ticket;
   __shared__ int s_ok;
-  const int n = p.ie - p.ib;
-  const long long step = (long long)p.state[0] + s;             // steps run before this one
-  const long long per_step = 2LL * n * w.nb;
-  if (threadIdx.x == 0) {
-    s_ticket = (long long)atomicAdd(w.ticket, 1ULL) - step * per_step;
-    s_ok = 1;
+  const int n = p.ie - p.ib, D = w.lag;
+  const int u = (int)(blockIdx.x / w.nb), bx = (int)(blockIdx.x - (unsigned)u * w.nb);
+  bool is_h;
+  int q;
+  if (u < D) {
+    is_h = false;
+    q = u;
+  } else if (u < D + 2 * (n - D)) {
+    const int r = u - D;
+    is_h = r & 1;
+    q = is_h ? r >> 1 : (r >> 1) + D;
+  } else {
+    is_h = true;
+    q = n - D + (u - D - 2 * (n - D));
   }
-  __syncthreads();
-  const long long t = s_ticket;
-  const int u = (int)(t / w.nb), bx = (int)(t - (long long)u * w.nb);
-  // unit u: 0 -> E(0); odd u < 2n - 1 -> E((u + 1) / 2); even u >= 2 -> H(u / 2 - 1); 2n - 1 -> H(n - 1)
-  const bool is_h = u == 2 * n - 1 || (u >= 2 && (u & 1) == 0);
-  const int q = u == 0 ? 0 : u == 2 * n - 1 ? n - 1 : (u & 1) ? (u + 1) / 2 : u / 2 - 1;
   if (!is_h) {
     v3_e_block<T, EXACT>(p, g, p.ib + q, bx, s);
     __threadfence();  // this thread's stores visible to the whole GPU ...
@@ -788,7 +792,8 @@ __global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSM 
     return;
   }
   if (threadIdx.x == 0) {
-    const int want = (int)((step + 1) * w.nb);
+    s_ok = 1;
+    const int want = (int)(((long long)p.state[0] + s + 1) * w.nb);  // counts after this step's E
     const long long t0 = clock64();
     for (int d = 0; d < 2 && q - d >= 0 && s_ok; ++d)
       while (ld_acquire(w.done + (q - d)) < want)

@@ -61,7 +61,7 @@ def drop_arrays(spec):
     the serving loop still reads (shape, steps, frequencies, windows, meta)
     stays."""
     spec.cb, spec.kdx, spec.twiddles = {}, {}, ()
-    spec.be = spec.ce = spec.bh = spec.ch = spec.j_src = None
+    spec.be = spec.ce = spec.bh = spec.ch = spec.j_src = spec.mat_idx = spec.mat_tab = None
     spec.meta = {k: v for k, v in spec.meta.items() if k != "core_mask"}
 
 

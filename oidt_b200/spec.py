@@ -53,6 +53,7 @@ class SimSpec:
     meta: dict = field(default_factory=dict)
     # optional (3D): the dt/eps grids as a one-byte material index [nx][ny][nz]
     # and its float64 table [nmat][3]; tab[idx] equals (cb['x'], cb['y'], cb['z'])
+    # (whoever changes cb drops these or rebuilds them)
     mat_idx: np.ndarray = None
     mat_tab: np.ndarray = None
 

@@ -104,6 +104,7 @@ def _graded(spec):
     rng = np.random.default_rng(11)
     for k in spec.cb:
         spec.cb[k] = spec.cb[k] * (1.0 + 0.01 * rng.random(spec.cb[k].shape))
+    spec.mat_idx = spec.mat_tab = None  # thousands of distinct triples: the grids themselves
     return spec
 
 
