@@ -508,7 +508,7 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 151 M-cell rib run")
     ap.add_argument("--ncu-case", choices=NCU_CASES, help="run one fixed workload for a profiler capture and exit")
     ap.add_argument("--case-steps", type=int, default=32)
-    ap.add_argument("--variant", default="vec", choices=("vec", "cell", "sweep"))
+    ap.add_argument("--variant", default="vec", choices=("vec", "wave", "cell", "sweep"))
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--precision", default="float32", choices=("float32", "float64"))
     args = ap.parse_args()
