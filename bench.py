@@ -236,24 +236,32 @@ def pinned_spec(spec, prec):
 def measure_slab2d(eng):
     """The 2D TMz slab case (400 x 200 cells, 2000 steps, float64, 21
     frequencies): device time of a whole run after a warm-up run, CUDA events
-    on the engine stream, exact and fast arithmetic."""
+    on the engine stream, exact and fast arithmetic, under the tile form
+    (a ring block of steps per launch, the default) and the per-cell
+    launches."""
     import torch
     from oidt_b200 import workloads as W
     spec = W.slab2d()
     st = torch.cuda.ExternalStream(eng.stream_handle(), device=eng.device)
     out = {"workload": "2D TMz slab %dx%d, %d steps, nf %d" % (spec.shape + (spec.nt, spec.nf)), "dtype": "f64"}
-    for arith in ("exact", "fast"):
-        job = eng.submit(spec, arith=arith, precision=np.float64)
-        job.run().sync()
-        job.reset()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        job.run()
-        e1.record(st)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        job.release()
-        out[arith] = {"ms_per_run": round(ms, 3), "gcell_updates_per_s": round(spec.ncells * spec.nt / ms / 1e6, 3)}
+    for variant in ("tile", "cell"):
+        for arith in ("exact", "fast"):
+            job = eng.submit(spec, arith=arith, precision=np.float64, variant=variant)
+            job.run().sync()
+            job.reset()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            job.run()
+            e1.record(st)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            job.release()
+            r = {"ms_per_run": round(ms, 3), "us_per_step": round(1e3 * ms / spec.nt, 3),
+                 "gcell_updates_per_s": round(spec.ncells * spec.nt / ms / 1e6, 3)}
+            if variant == "tile":
+                out[arith] = r
+            else:
+                out.setdefault("per_cell_launches", {})[arith] = r
     return out
 
 
@@ -508,7 +516,7 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 151 M-cell rib run")
     ap.add_argument("--ncu-case", choices=NCU_CASES, help="run one fixed workload for a profiler capture and exit")
     ap.add_argument("--case-steps", type=int, default=32)
-    ap.add_argument("--variant", default="vec", choices=("vec", "wave", "cell", "sweep"))
+    ap.add_argument("--variant", default="auto", choices=("auto", "vec", "wave", "cell", "sweep", "tile"))
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--precision", default="float32", choices=("float32", "float64"))
     args = ap.parse_args()

@@ -42,18 +42,22 @@
 #include "kernels.cuh"
 #include "sweep3d.cuh"
 #include "vec3d.cuh"
+#include "tile2d.cuh"
 
 using namespace oidt;
 
 namespace {
 
 constexpr int kDefaultRing = 32;
-constexpr int kFoldF = 7;  // frequencies per fold thread (41 = 6 x 7 - 1)
+constexpr int kFoldF = 7;  // frequencies per fold thread in 3D (41 = 6 x 7 - 1); 2D: one
 constexpr int kBlock3Z = 32, kRowsDefault = 4;  // 3D per-cell tile: 32 (k) x rows (j), rows 2, 4 or 8
 constexpr int kBlock2 = 128;
 constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
 constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread box
 constexpr int kVariantCell = 0, kVariantSweep = 1, kVariantVec = 2, kVariantWave = 3;  // oidt_job_desc.reserved[0]
+constexpr int kVariantTile = 4;  // 2D: tiles advanced up to kTileHaloMax steps per launch in shared memory
+constexpr int kTileMaxBlocks = 1024;  // tiles of a cooperative (several sub-block) launch at most
+constexpr size_t kTileSmemMax = 227 * 1024;  // shared memory of a tile block at most
 
 // ---------------------------------------------------------------------------
 // Line probe (wave-impedance recording): after every step, colocated Ey, Ez,
@@ -173,7 +177,7 @@ template <typename T> struct FoldParams {
   double2 *acc;
   const double *tw[4];  // cosE sinE cosH sinH
   int wlo0, whi0, wlo1, whi1;
-  const int *state;
+  int *state;  // state[0]: absolute step of ring slot 0; state[2]: fold blocks done
 };
 
 template <typename T, bool EXACT>
@@ -208,15 +212,21 @@ __device__ __forceinline__ double coloc(const FoldParams<T> &fp, int port, int c
   }
 }
 
-// One block: 128 window cells x kFoldF frequencies of one (port, component).
+// One block: 128 window cells x FF frequencies of one (port, component).  3D
+// planes have thousands of window cells: FF = kFoldF frequencies a thread
+// share each sample load; a 2D port line has a few hundred, so FF = 1 there
+// (fifteen thousand short accumulation chains rather than two thousand long ones).
 // The block's twiddles for up to kFoldChunk steps are staged in shared memory
-// (every thread uses the same values), accumulators stay in registers.
+// (every thread uses the same values), and so are a thread's colocated
+// samples of those steps (their loads issued together rather than one ring
+// latency per step); accumulators stay in registers.
 constexpr int kFoldChunk = 32;
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, int FF>
 __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
   pdl_wait();
   using A = Ar<double, EXACT>;
-  __shared__ double2 tw[kFoldChunk][kFoldF];
+  __shared__ double2 tw[kFoldChunk][FF];
+  __shared__ double xs[kFoldChunk][128];
   const int wj = fp.whi1 - fp.wlo1;
   const int wi = fp.mode == OIDT_MODE_YEE3D ? fp.whi0 - fp.wlo0 : 1;
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -226,13 +236,13 @@ __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
   const int port = blockIdx.z / fp.ncomp, comp = blockIdx.z % fp.ncomp;
   const bool hcomp = fp.mode == OIDT_MODE_YEE3D ? comp >= 2 : comp == 1;
   const double *cs = fp.tw[hcomp ? 2 : 0], *sn = fp.tw[hcomp ? 3 : 1];
-  const int f0 = blockIdx.y * kFoldF;
-  const int nfc = min(kFoldF, fp.nf - f0);
+  const int f0 = blockIdx.y * FF;
+  const int nfc = min(FF, fp.nf - f0);
   const long long cell = fp.mode == OIDT_MODE_YEE3D ? (long long)i * fp.ny + j : j;
   double2 *acc = fp.acc + (((long long)port * fp.ncomp + comp) * fp.nf + f0) * fp.plane + cell;
-  double re[kFoldF], im[kFoldF];
+  double re[FF], im[FF];
 #pragma unroll
-  for (int f = 0; f < kFoldF; ++f) {
+  for (int f = 0; f < FF; ++f) {
     re[f] = 0.0;
     im[f] = 0.0;
     if (active && f < nfc) { double2 a = acc[f * fp.plane]; re[f] = a.x; im[f] = a.y; }
@@ -241,17 +251,21 @@ __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
   for (int s0 = 0; s0 < count; s0 += kFoldChunk) {
     const int sc = min(kFoldChunk, count - s0);
     __syncthreads();
-    for (int t = threadIdx.x; t < sc * kFoldF; t += blockDim.x) {
-      const int ss = t / kFoldF, f = t % kFoldF;
+    for (int t = threadIdx.x; t < sc * FF; t += blockDim.x) {
+      const int ss = t / FF, f = t % FF;
       const long long idx = (long long)(f0 + f) * fp.nt + n0 + s0 + ss;
       tw[ss][f] = f < nfc ? make_double2(__ldg(cs + idx), __ldg(sn + idx)) : make_double2(0.0, 0.0);
+    }
+    if (active) {
+#pragma unroll 8
+      for (int ss = 0; ss < sc; ++ss) xs[ss][threadIdx.x] = coloc<T, EXACT>(fp, port, comp, s0 + ss, i, j);
     }
     __syncthreads();
     if (active) {
       for (int ss = 0; ss < sc; ++ss) {
-        const double x = coloc<T, EXACT>(fp, port, comp, s0 + ss, i, j);
+        const double x = xs[ss][threadIdx.x];
 #pragma unroll
-        for (int f = 0; f < kFoldF; ++f) {
+        for (int f = 0; f < FF; ++f) {
           const double2 t = tw[ss][f];
           re[f] = A::add(re[f], A::mul(x, t.x));
           im[f] = A::sub(im[f], A::mul(x, t.y));
@@ -261,14 +275,18 @@ __global__ void __launch_bounds__(128) k_fold(FoldParams<T> fp, int count) {
   }
   if (active) {
 #pragma unroll
-    for (int f = 0; f < kFoldF; ++f)
+    for (int f = 0; f < FF; ++f)
       if (f < nfc) acc[f * fp.plane] = make_double2(re[f], im[f]);
   }
-}
-
-__global__ void k_bump(int *state, int count) {
-  pdl_wait();
-  if (threadIdx.x == 0 && blockIdx.x == 0) state[0] += count;
+  // the last block to finish advances the ring's step (every block has read it by then)
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+    if (atomicAdd(reinterpret_cast<unsigned *>(fp.state + 2), 1u) == nb - 1) {
+      fp.state[2] = 0;
+      fp.state[0] += count;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -288,6 +306,9 @@ struct Layout {
 int ncomp_of(int mode) { return mode == OIDT_MODE_YEE3D ? 4 : 2; }
 int nslot_of(int mode) { return mode == OIDT_MODE_YEE3D ? 6 : 3; }
 bool is_e(int f) { return f <= EZ; }
+// psi buffers of a field: the plane sweep double-buffers E psi (it updates H
+// psi in place); the 2D tile form double-buffers every psi array.
+int psi_bufs(int nbuf, int variant, int f) { return nbuf == 2 && (is_e(f) || variant == kVariantTile) ? 2 : 1; }
 
 // (field, slab axis) pairs with CPML psi arrays per solver, in the reference's
 // PSI_<F>_<A> naming.
@@ -328,6 +349,7 @@ struct JobPlan {
   size_t off_mat, off_mtab;       // material index [nx][ny][nzp] and table [256][4] (3D, optional)
   bool mat;
   size_t off_wave;                // ordered form: E-block counts per plane (after 8 spare bytes)
+  size_t off_tile;                // 2D tile form: sub-blocks completed per tile [kTileMaxBlocks]
   size_t off_pow;                 // port power [nf] complex float64
   long long N, plane;
   int K, esz, nzp, nbuf, variant, L, nitems;
@@ -481,15 +503,22 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   } else if (d->probe[1] != 0 || d->probe[2] != 0) {
     return bad("probe[1..2] must be 0 without a probe");
   }
-  if (d->reserved[0] < kVariantCell || d->reserved[0] > kVariantWave) return bad("reserved[0]: launch form 0 to 3");
+  if (is3 && (d->reserved[0] < kVariantCell || d->reserved[0] > kVariantWave))
+    return bad("reserved[0]: 3D launch form 0 to 3");
+  if (!is3 && d->reserved[0] != kVariantCell && d->reserved[0] != kVariantTile)
+    return bad("reserved[0]: 2D launch form 0 (per-cell) or 4 (tiles)");
   if (d->reserved[1] != 0 && d->reserved[1] != 1) return bad("reserved[1]: 0 or 1");
-  const int variant = is3 ? d->reserved[0] : kVariantCell;
+  const int variant = d->reserved[0];
+  if (variant == kVariantTile && tile2d_smem(d->precision == OIDT_F32 ? 4 : 8, P) > kTileSmemMax)
+    return bad("tile form: num_cpml too large for a block's shared memory");
+  if (variant == kVariantTile && ((long long)d->nx * d->ny > 0x7fffffffLL || (long long)d->nx * P > 0x7fffffffLL))
+    return bad("tile form: the grid holds 2^31 or more cells");
   const int rows = d->reserved[2] == 0 ? kRowsDefault : d->reserved[2];
   if (rows != 2 && rows != 4 && rows != 8) return bad("reserved[2]: tile rows 0 (default), 2, 4 or 8");
   if (d->reserved[2] != 0 && !(is3 && variant == kVariantCell))
     return bad("reserved[2] (tile rows) applies to the 3D per-cell form");
-  if (d->reserved[3] < 0 || (d->reserved[3] != 0 && !(is3 && variant == kVariantSweep)))
-    return bad("reserved[3] (march depth) is >= 0 and applies to the 3D plane sweep");
+  if (d->reserved[3] < 0 || (d->reserved[3] != 0 && !(is3 ? variant == kVariantSweep : variant == kVariantTile)))
+    return bad("reserved[3] is >= 0: the 3D plane sweep's march depth or the 2D tile form's steps per launch");
   const int esz = d->precision == OIDT_F32 ? 4 : 8;
   const int nzp = is3 ? (int)align_up(d->nz, 4) : 1;
   const long long N = (long long)d->nx * d->ny * nzp;
@@ -497,7 +526,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   int K = d->ring_steps > 0 ? d->ring_steps : kDefaultRing;
   if (K > 4096) return bad("ring_steps too large");
   if (variant == kVariantSweep && (K & 1)) ++K;  // graphs of the sweep end on the parity they start
-  const int nbuf = variant == kVariantSweep ? 2 : 1;
+  const int nbuf = variant == kVariantSweep || variant == kVariantTile ? 2 : 1;
   const bool vec_rows = variant == kVariantVec || variant == kVariantWave;  // the vector form's kernels
   const int psi_pitch = vec_rows ? nzp : d->nz;
   if (variant == kVariantWave) {  // block counts per plane and step stay in 32-bit counters
@@ -527,7 +556,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->off_bh = L.take(P * esz);
   pl->off_ch = L.take(P * esz);
   for (auto fa : psi_pairs(d->mode))
-    for (int b = 0; b < (is_e(fa.first) ? nbuf : 1); ++b)
+    for (int b = 0; b < psi_bufs(nbuf, variant, fa.first); ++b)
       for (int sd = 0; sd < 2; ++sd)
         pl->off_psi[b][fa.first][fa.second][sd] = L.take(psi_elems(d->mode, fa.second, d->nx, d->ny, d->nz, P, psi_pitch) * esz);
   pl->off_jsrc = L.take((size_t)d->nt * esz);
@@ -542,6 +571,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
     pl->off_mtab = L.take((size_t)256 * 4 * esz);
   }
   if (variant == kVariantWave) pl->off_wave = L.take(8 + (size_t)4 * (d->ie - d->ib));
+  if (variant == kVariantTile) pl->off_tile = L.take((size_t)4 * kTileMaxBlocks);
   if (d->probe[0] == 1) {
     pl->probe_bytes = (size_t)4 * d->nt * d->nx * esz;
     pl->off_probe = L.take(pl->probe_bytes);
@@ -584,6 +614,10 @@ struct Job {
   long long steps_enqueued = 0;
   bool busy = false;
   long long wait_cycles = kWaitCycles;  // plane sweep: bound on its tile-load waits
+  TileArgs tile{};                      // 2D tile form: tile extents, tiles along y, halo
+  int tile_blocks = 0;                  // ... blocks (tiles) of a launch
+  bool tile_coop = false;               // ... a ring block is one cooperative launch of sub-blocks
+  size_t tile_smem = 0;                 // ... shared memory of a block
 };
 
 constexpr int kAuxStreams = 64;  // a served request is two jobs; the mix keeps ~40 active
@@ -603,6 +637,8 @@ struct oidt_ctx {
   std::mutex mu;
   std::string err;
   long long launches = 0;
+  int sms = 148;      // streaming multiprocessors of the device
+  bool coop = false;  // ... and whether it takes cooperative launches
 };
 
 namespace {
@@ -709,7 +745,7 @@ template <typename T> void fill_params(Job *J) {
     p.wait_cycles = J->wait_cycles;
     for (auto fa : psi_pairs(d.mode))
       for (int sd = 0; sd < 2; ++sd) {
-        const bool two = is_e(fa.first) && pl.nbuf == 2;
+        const bool two = psi_bufs(pl.nbuf, pl.variant, fa.first) == 2;
         p.psi[fa.first][fa.second][sd] = reinterpret_cast<T *>(m + pl.off_psi[two ? bb : 0][fa.first][fa.second][sd]);
         p.psin[fa.first][fa.second][sd] = p.psi[fa.first][fa.second][sd];  // in place
       }
@@ -729,7 +765,7 @@ template <typename T> void fill_params(Job *J) {
     v = p;
     if (pl.nbuf == 2) {
       for (auto fa : psi_pairs(d.mode))
-        if (is_e(fa.first))
+        if (psi_bufs(pl.nbuf, pl.variant, fa.first) == 2)
           for (int sd = 0; sd < 2; ++sd)
             v.psin[fa.first][fa.second][sd] = reinterpret_cast<T *>(m + pl.off_psi[bb ^ 1][fa.first][fa.second][sd]);
       v.tmap_f = m + pl.off_tmaps + (size_t)bb * 6 * 128;
@@ -914,6 +950,40 @@ template <typename T, bool EXACT> void v3_wave(Job *J, bool pdl, const Params<T>
   else k_v3_wave<T, EXACT><<<grd, blk, 0, st>>>(p, g, w, s);
 }
 
+// One launch of the 2D tile form (k_2d_tile): steps s0 .. s0 + cnt - 1 of a
+// ring block, read from buffer p.f / p.psi, owned cells written to p.fn /
+// p.psin.
+// cnt > halo: one cooperative launch of ceil(cnt / halo) sub-blocks.
+template <typename T, bool EXACT>
+void tile_launch(bool pdl, Job *J, const Params<T> &p, int s0, int cnt, cudaStream_t st) {
+  void (*kern)(Params<T>, TileArgs) =
+      p.mode == OIDT_MODE_TM2 ? k_2d_tile<T, EXACT, OIDT_MODE_TM2> : k_2d_tile<T, EXACT, OIDT_MODE_TE2>;
+  TileArgs a = J->tile;
+  a.s0 = s0;
+  a.cnt = cnt;
+  a.epoch = reinterpret_cast<int *>(J->mem + J->pl.off_tile);
+  if (cnt > a.halo) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(J->tile_blocks);
+    cfg.blockDim = dim3(kTileThreads);
+    cfg.dynamicSmemBytes = J->tile_smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, p, a);
+  } else if (pdl) {
+    launch_step_kernel(kern, dim3(J->tile_blocks), dim3(kTileThreads), J->tile_smem, st, p, a);
+  } else {
+    kern<<<J->tile_blocks, kTileThreads, J->tile_smem, st>>>(p, a);
+  }
+}
+
+// Launches of the 2D tile form for cnt steps: up to halo steps each.
+int tile_launches(const Job *J, int cnt) { return (cnt + J->tile.halo - 1) / J->tile.halo; }
+
 template <typename T> size_t sweep_smem() { return sweep_smem_bytes<T, EYB, EZB, ST>(); }
 
 template <typename T, bool EXACT>
@@ -979,24 +1049,56 @@ template <typename T, bool EXACT> void launch_fold(oidt_ctx *ctx, Job *J, int co
   FoldParams<T> &fp = fold_of<T>(J);
   const int wj = fp.whi1 - fp.wlo1;
   const int wi = J->d.mode == OIDT_MODE_YEE3D ? fp.whi0 - fp.wlo0 : 1;
-  dim3 grd((wi * wj + 127) / 128, (fp.nf + kFoldF - 1) / kFoldF, 2 * fp.ncomp);
-  launch_step_kernel(k_fold<T, EXACT>, grd, dim3(128), 0, st, fp, count);
-  launch_step_kernel(k_bump, dim3(1), dim3(32), 0, st, reinterpret_cast<int *>(J->mem + J->pl.off_state), count);
-  ctx->launches += 2;
+  if (J->d.mode == OIDT_MODE_YEE3D) {
+    dim3 grd((wi * wj + 127) / 128, (fp.nf + kFoldF - 1) / kFoldF, 2 * fp.ncomp);
+    launch_step_kernel(k_fold<T, EXACT, kFoldF>, grd, dim3(128), 0, st, fp, count);
+  } else {
+    dim3 grd((wi * wj + 127) / 128, fp.nf, 2 * fp.ncomp);
+    launch_step_kernel(k_fold<T, EXACT, 1>, grd, dim3(128), 0, st, fp, count);
+  }
+  ctx->launches += 1;
 }
 
 int steps_flip(const Job *J) { return J->pl.variant == kVariantSweep ? 1 : 0; }
+
+// Buffer parity change of a cnt-step block: the plane sweep flips every step,
+// the tile form every launch.
+int block_flip(const Job *J, int cnt) {
+  if (J->pl.variant == kVariantSweep) return cnt & 1;
+  if (J->pl.variant == kVariantTile) return tile_launches(J, cnt) & 1;
+  return 0;
+}
+
+// Steps 0..cnt-1 of a K-step block starting on buffer parity par.
+template <typename T, bool EXACT> void launch_steps(oidt_ctx *ctx, Job *J, int cnt, int par, cudaStream_t st) {
+  if (J->pl.variant == kVariantTile) {  // each sub-block reads one buffer and writes the other
+    if (J->tile_coop) {
+      tile_launch<T, EXACT>(true, J, views<T>(J)[par], 0, cnt, st);
+      ctx->launches += 1;
+      return;
+    }
+    const int nl = tile_launches(J, cnt);
+    for (int l = 0; l < nl; ++l) {
+      const int s0 = l * J->tile.halo;
+      tile_launch<T, EXACT>(true, J, views<T>(J)[par ^ (l & 1)], s0, std::min(J->tile.halo, cnt - s0), st);
+    }
+    ctx->launches += nl;
+    return;
+  }
+  const int flip = steps_flip(J);
+  for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, par ^ (flip & s), st);
+}
 
 // The job's K-step block starting on buffer parity par (its steps, then its
 // DFT fold) as a CUDA graph, captured on stream st at first use.  Capture
 // enqueues nothing, so st may hold work of other jobs.
 template <typename T, bool EXACT> int job_graph(oidt_ctx *ctx, Job *J, int par, cudaStream_t st) {
   if (J->graph[par]) return OIDT_OK;
-  const int K = J->pl.K, flip = steps_flip(J);
+  const int K = J->pl.K;
   cudaGraph_t g;
   const long long before = ctx->launches;
   CU(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  for (int s = 0; s < K; ++s) launch_step<T, EXACT>(ctx, J, s, par ^ (flip & s), st);
+  launch_steps<T, EXACT>(ctx, J, K, par, st);
   launch_fold<T, EXACT>(ctx, J, K, st);
   CU(ctx, cudaStreamEndCapture(st, &g));
   const cudaError_t ie = cudaGraphInstantiate(&J->graph[par], g, 0);
@@ -1011,7 +1113,6 @@ template <typename T, bool EXACT> int advance_t(oidt_ctx *ctx, Job *J, int nstep
   cudaStream_t st = ctx->stream;
   CU(ctx, cudaStreamWaitEvent(st, J->ready, 0));
   const int K = J->pl.K;
-  const int flip = steps_flip(J);
   int left = nsteps;
   while (left > 0) {
     const int cnt = std::min(K, left);
@@ -1022,10 +1123,10 @@ template <typename T, bool EXACT> int advance_t(oidt_ctx *ctx, Job *J, int nstep
       CU(ctx, cudaGraphLaunch(J->graph[par], st));
       ctx->launches += J->graph_launches;
     } else {
-      for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, par ^ (flip & s), st);
+      launch_steps<T, EXACT>(ctx, J, cnt, par, st);
       launch_fold<T, EXACT>(ctx, J, cnt, st);
     }
-    J->parity ^= flip & cnt;
+    J->parity ^= block_flip(J, cnt);
     left -= cnt;
   }
   CU(ctx, cudaGetLastError());
@@ -1063,15 +1164,14 @@ template <typename T, bool EXACT> int batch_block(oidt_ctx *ctx, std::vector<Job
   for (int b = 0; b < (int)js.size(); ++b) {
     Job *J = js[b];
     cudaStream_t sb = ctx->aux[b % na];
-    const int flip = steps_flip(J);
     if (full && J->d.reserved[1] == 0) {
       CU(ctx, cudaGraphLaunch(J->graph[J->parity], sb));
       ctx->launches += J->graph_launches;
     } else {
-      for (int s = 0; s < cnt; ++s) launch_step<T, EXACT>(ctx, J, s, J->parity ^ (flip & s), sb);
+      launch_steps<T, EXACT>(ctx, J, cnt, J->parity, sb);
       launch_fold<T, EXACT>(ctx, J, cnt, sb);
     }
-    J->parity ^= flip & cnt;
+    J->parity ^= block_flip(J, cnt);
   }
   for (int a = 0; a < na; ++a) {
     CU(ctx, cudaEventRecord(ctx->join[a], ctx->aux[a]));
@@ -1127,6 +1227,35 @@ template <typename T, bool EXACT> int profile_t(oidt_ctx *ctx, Job *J, int nstep
   CU(ctx, cudaStreamWaitEvent(st, J->ready, 0));
   std::vector<cudaEvent_t> ev(2 * (2 * nsteps + 2));
   for (auto &e : ev) CU(ctx, cudaEventCreate(&e));
+  if (J->pl.variant == kVariantTile) {  // launches of up to halo steps: time per step as the E half, H half = 0
+    const int nl = tile_launches(J, nsteps);
+    cudaEventRecord(ev[0], st);
+    if (J->tile_coop) {
+      tile_launch<T, EXACT>(false, J, views<T>(J)[J->parity], 0, nsteps, st);
+    } else {
+      for (int l = 0; l < nl; ++l) {
+        const int s0 = l * J->tile.halo;
+        tile_launch<T, EXACT>(false, J, views<T>(J)[J->parity ^ (l & 1)], s0, std::min(J->tile.halo, nsteps - s0), st);
+      }
+    }
+    cudaEventRecord(ev[1], st);
+    launch_fold<T, EXACT>(ctx, J, nsteps, st);
+    cudaEventRecord(ev[2], st);
+    ctx->launches += J->tile_coop ? 1 : nl;
+    J->parity ^= nl & 1;
+    CU(ctx, cudaGetLastError());
+    CU(ctx, cudaStreamSynchronize(st));
+    float a = 0, fo = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&fo, ev[1], ev[2]);
+    ms[0] = a / nsteps;
+    ms[1] = 0;
+    ms[2] = fo;
+    for (auto &e : ev) cudaEventDestroy(e);
+    J->steps_enqueued += nsteps;
+    CU(ctx, cudaEventRecord(J->done, st));
+    return OIDT_OK;
+  }
   const bool sweep = J->pl.variant == kVariantSweep;
   int q = 0;
   for (int s = 0; s < nsteps; ++s) {
@@ -1222,6 +1351,76 @@ int set_sweep_attrs() {
   return std::max(1, per_sm) * std::max(1, sms);
 }
 
+// The 2D tile kernels take tile2d_smem(esz, P) bytes of shared memory a block, at
+// most kTileSmemMax.
+template <typename T, bool EXACT, int MODE> void tile_attrs_of() {
+  cudaFuncSetAttribute(k_2d_tile<T, EXACT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmemMax);
+}
+
+void set_tile_attrs() {
+  tile_attrs_of<float, false, OIDT_MODE_TM2>();
+  tile_attrs_of<float, true, OIDT_MODE_TM2>();
+  tile_attrs_of<double, false, OIDT_MODE_TM2>();
+  tile_attrs_of<double, true, OIDT_MODE_TM2>();
+  tile_attrs_of<float, false, OIDT_MODE_TE2>();
+  tile_attrs_of<float, true, OIDT_MODE_TE2>();
+  tile_attrs_of<double, false, OIDT_MODE_TE2>();
+  tile_attrs_of<double, true, OIDT_MODE_TE2>();
+}
+
+// The tile form's split of a job.  A held tile has at most kTileThreads
+// cells.  For each steps-per-launch h (the halo: at most min(8, ring steps),
+// or the descriptor's reserved[3]), the tiling with the fewest waves of blocks
+// over the SMs, then the fewest cells held in all; then the h with the least
+// estimated time per step: about 0.5 us per step and wave, and about 2 us of
+// launch overhead per launch.
+void tile_plan(Job *J, int sms) {
+  const oidt_job_desc &d = J->d;
+  const int nx = d.nx, ny = d.ny;
+  const int hmax = std::min(kTileHaloMax, J->pl.K);
+  const int h0 = d.reserved[3] > 0 ? std::min(d.reserved[3], hmax) : 1;
+  const int h1 = d.reserved[3] > 0 ? h0 : hmax;
+  double best_t = 1e30;
+  for (int h = h0; h <= h1; ++h) {
+    long long bk0 = -1, bk1 = 0;
+    TileArgs bt{};
+    int bb = 0;
+    // a held tile of (ti + 2h) x (tj + 2h) <= kTileThreads cells (clipped at the grid's edges)
+    for (int ti = 1; ti <= nx; ++ti) {
+      const int hi = std::min(nx, ti + 2 * h);
+      if (hi > kTileThreads) break;
+      const int gi = (nx + ti - 1) / ti;
+      if (ti > 1 && (nx + ti - 2) / (ti - 1) == gi) continue;  // the smallest ti of this tile count
+      // the widest owned tile, then the narrowest with as many tiles along y
+      const int tjmax = ny * hi <= kTileThreads ? ny : std::min(ny, kTileThreads / hi - 2 * h);
+      if (tjmax < 1) continue;
+      const int gjn = (ny + tjmax - 1) / tjmax;
+      {
+        const int tj = (ny + gjn - 1) / gjn;
+        const long long tiles = (long long)gi * ((ny + tj - 1) / tj);
+        const long long cells = (long long)std::min(nx, ti + 2 * h) * std::min(ny, tj + 2 * h);
+        const long long k0 = (tiles + sms - 1) / sms, k1 = tiles * cells;
+        if (bk0 < 0 || k0 < bk0 || (k0 == bk0 && k1 < bk1)) {
+          bk0 = k0;
+          bk1 = k1;
+          bt.ti = ti;
+          bt.tj = tj;
+          bt.gj = (ny + tj - 1) / tj;
+          bb = (int)tiles;
+        }
+      }
+    }
+    if (bk0 < 0) continue;
+    const double t = 0.5 * (double)bk0 + 2.0 / h;
+    if (t < best_t) {
+      best_t = t;
+      J->tile = bt;
+      J->tile.halo = h;
+      J->tile_blocks = bb;
+    }
+  }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1281,6 +1480,11 @@ int32_t oidt_create(int32_t device, uint64_t hbm_budget, oidt_ctx **out) {
   }
   cudaEventCreateWithFlags(&ctx->fork, cudaEventDisableTiming);
   g_sweep_slots = set_sweep_attrs();
+  set_tile_attrs();
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  ctx->coop = coop != 0;
   size_t fr = 0, tot = 0;
   cudaMemGetInfo(&fr, &tot);
   ctx->budget = hbm_budget ? hbm_budget : (uint64_t)(0.9 * (double)fr);
@@ -1347,6 +1551,14 @@ int32_t oidt_job_create(oidt_ctx *ctx, const oidt_job_desc *desc, uint64_t *job)
   Job *J = new Job();
   J->d = *desc;
   J->pl = pl;
+  if (pl.variant == kVariantTile) {
+    tile_plan(J, ctx->sms);
+    J->tile_smem = tile2d_smem(pl.esz, desc->num_cpml);
+    // a ring block in one launch where every tile is resident at once and a tile's
+    // halo reaches its 8 neighbours only
+    J->tile_coop = ctx->coop && J->tile_blocks <= std::min(ctx->sms, kTileMaxBlocks) &&
+                   J->tile.halo <= std::min(J->tile.ti, J->tile.tj) && J->pl.K > J->tile.halo;
+  }
   if (cudaMallocAsync(reinterpret_cast<void **>(&J->mem), pl.total, ctx->upload) != cudaSuccess) {
     delete J;
     cudaGetLastError();
@@ -1434,7 +1646,7 @@ int32_t oidt_job_sync(oidt_ctx *ctx, uint64_t job, int32_t timeout_ms) {
     if (cudaMemcpy(flags, state, sizeof flags, cudaMemcpyDeviceToHost) == cudaSuccess && flags[1])
       return fail(ctx, OIDT_ERR_TIMEOUT,
                   "a kernel's bounded wait expired (device flag %d: 1 = the plane sweep's tile loads, "
-                  "2 = the ordered form's plane order)", flags[1]);
+                  "2 = the ordered form's plane order, 3 = the 2D tile form's neighbour tiles)", flags[1]);
   }
   return rc;
 }
@@ -1736,7 +1948,7 @@ int32_t oidt_job_read_psi(oidt_ctx *ctx, uint64_t job, int32_t field, int32_t ax
   if (nbytes < need) return fail(ctx, OIDT_ERR_INVALID, "output needs %zu bytes", need);
   int rc = read_common(ctx, J);
   if (rc) return rc;
-  const int b = (is_e(field) && J->pl.nbuf == 2) ? J->parity : 0;
+  const int b = psi_bufs(J->pl.nbuf, J->pl.variant, field) == 2 ? J->parity : 0;
   const unsigned char *src = J->mem + J->pl.off_psi[b][field][axis][side];
   const bool pitched = J->d.mode == OIDT_MODE_YEE3D && axis != AZ && J->pl.psi_pitch != J->d.nz;
   if (pitched) {  // rows of nz cells out of rows of psi_pitch cells
@@ -1773,7 +1985,7 @@ int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
   for (int b = 0; b < pl.nbuf; ++b)
     for (int f : fields_of(J->d.mode)) CU(ctx, cudaMemsetAsync(J->mem + pl.off_f[b][f], 0, pl.N * pl.esz, st));
   for (auto fa : psi_pairs(J->d.mode))
-    for (int b = 0; b < (is_e(fa.first) ? pl.nbuf : 1); ++b)
+    for (int b = 0; b < psi_bufs(pl.nbuf, pl.variant, fa.first); ++b)
       for (int sd = 0; sd < 2; ++sd)
         CU(ctx, cudaMemsetAsync(J->mem + pl.off_psi[b][fa.first][fa.second][sd], 0,
                                 psi_elems(J->d.mode, fa.second, J->d.nx, J->d.ny, J->d.nz, J->d.num_cpml,
@@ -1784,6 +1996,8 @@ int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
   if (pl.probe_bytes) CU(ctx, cudaMemsetAsync(J->mem + pl.off_probe, 0, pl.probe_bytes, st));
   if (pl.variant == kVariantWave)  // the ordered form's counters restart with the steps
     CU(ctx, cudaMemsetAsync(J->mem + pl.off_wave, 0, 8 + (size_t)4 * (J->d.ie - J->d.ib), st));
+  if (pl.variant == kVariantTile)  // the tiles' sub-block counters: equal (zero) again
+    CU(ctx, cudaMemsetAsync(J->mem + pl.off_tile, 0, (size_t)4 * kTileMaxBlocks, st));
   CU(ctx, cudaEventRecord(J->done, st));
   J->busy = true;
   J->steps_enqueued = 0;

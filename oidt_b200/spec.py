@@ -90,7 +90,14 @@ class JobDesc(C.Structure):
     ]
 
 
-VARIANTS = {"cell": 0, "sweep": 1, "vec": 2, "wave": 3}
+VARIANTS = {"cell": 0, "sweep": 1, "vec": 2, "wave": 3, "tile": 4}
+
+
+def resolve_variant(spec: "SimSpec", variant: str) -> str:
+    """'auto': the vector form in 3D, the tile form in 2D."""
+    if variant != "auto":
+        return variant
+    return "vec" if spec.mode == "yee3d" else "tile"
 
 
 def power_window(spec: SimSpec):
@@ -102,17 +109,22 @@ def power_window(spec: SimSpec):
         return tuple(map(tuple, w)) if w else ((spec.win_lo[0], spec.win_hi[0]), (spec.win_lo[1], spec.win_hi[1]))
     return tuple(w) if w else (spec.win_lo[1], spec.win_hi[1])
 
-
-def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "vec",
-            graphs: bool = True, rows: int = 0, march_depth: int = 0, material: bool = True):
+def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "auto",
+            graphs: bool = True, rows: int = 0, march_depth: int = 0, material: bool = True, tile_steps: int = 0):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
     ``keepalive`` must outlive the ``oidt_job_create`` call.
 
-    ``variant`` (3D only): 'vec' (default) -- the E-half / H-half launches
-    with four cells per thread along z and 16-byte accesses; 'wave' -- the
-    same code in one launch per step, E and H half-steps ordered plane by
-    plane; 'cell' -- the half-steps with one cell per thread; 'sweep' -- one
-    plane-sweep launch per step (E and H fused, TMA-staged tiles).  2D jobs always use the per-cell launches.  ``graphs=False``
+    ``variant``: 'auto' (default) picks 'vec' in 3D and 'tile' in 2D.  3D: 'vec' -- the E-half / H-half
+    launches with four cells per thread along z and 16-byte accesses;
+    'wave' -- the same code in one launch per step, E and H half-steps
+    ordered plane by plane; 'cell' -- the half-steps with one cell per
+    thread; 'sweep' -- one plane-sweep launch per step (E and H fused,
+    TMA-staged tiles).  2D: 'cell' -- the E-half / H-half launches with one
+    cell per thread; 'tile' -- up to 8 steps per launch, each block advancing
+    a tile of the grid (and a halo around it) in shared memory.
+    ``tile_steps`` (2D tile form): steps per launch, 1 to 8 (0 = the
+    engine's estimate).
+    ``graphs=False``
     launches every step directly instead of replaying K-step CUDA graphs.
     ``rows`` (3D per-cell form): tile rows of a block, 2, 4 or 8 (0 = 4);
     ``march_depth`` (3D plane sweep): x-planes per work item (0 = the
@@ -169,10 +181,10 @@ def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int 
     tw = [arr(t, np.float64) for t in spec.twiddles]
     d.cos_e, d.sin_e, d.cos_h, d.sin_h = tw
     d.ring_steps = ring_steps
-    d.reserved[0] = VARIANTS[variant]
+    d.reserved[0] = VARIANTS[resolve_variant(spec, variant)]
     d.reserved[1] = 0 if graphs else 1
     d.reserved[2] = int(rows)
-    d.reserved[3] = int(march_depth)
+    d.reserved[3] = int(march_depth) or int(tile_steps)
     probe = spec.meta.get("probe")  # (y, z) of a 3D line probe along x
     if probe is not None:
         d.probe[0], d.probe[1], d.probe[2] = 1, int(probe[0]), int(probe[1])

@@ -81,8 +81,8 @@ class Tuner:
     def choose(self, spec: SimSpec, precision=None, arith: str = "fast", ring_steps: int = 32) -> dict:
         """The ``submit`` keywords for ``spec``: the cached choice of its shape
         key, measured now if the key is new."""
-        if spec.mode != "yee3d":
-            return dict(DEFAULT)
+        if spec.mode != "yee3d":  # 2D: the tile form
+            return dict(DEFAULT, variant="auto")
         key = shape_key(spec, precision, arith, ring_steps)
         with self._lock:
             hit = self.table.get(key)

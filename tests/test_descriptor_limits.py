@@ -59,7 +59,8 @@ MUT3 = [
 
 MUT2 = [
     ("nz", 2), ("src_field", 0), ("src_field", 5), ("kdx[0]", None), ("cb[2]", None),
-    ("port_pos[1]", 59), ("win_hi[1]", 50), ("probe[0]", 1), ("reserved[2]", 4), ("reserved[3]", 1),
+    ("port_pos[1]", 59), ("win_hi[1]", 50), ("probe[0]", 1), ("reserved[2]", 4), ("reserved[3]", -1),
+    ("reserved[0]", 1), ("reserved[0]", 2), ("reserved[0]", 5),
 ]
 
 

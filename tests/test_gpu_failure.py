@@ -105,3 +105,36 @@ def test_sweep_tile_wait_expiry_is_reported_and_recoverable():
         np.testing.assert_array_equal(job.field(f), v)
     job.release()
     eng.close()
+
+
+def test_tile_neighbour_wait_expiry_is_reported_and_recoverable():
+    """The 2D tile form's cooperative launches wait, between sub-blocks, for
+    the neighbour tiles' counters; the waits are bounded in the kernel.  With
+    a bound of one cycle they run out wherever a neighbour tile is still
+    computing when a tile reaches its wait (144 tiles, hundreds of waits a
+    launch); the tile records the expiry and goes on, later waits of the
+    launch give up at once, and the launch ends.  oidt_job_sync reports
+    OIDT_ERR_TIMEOUT; the context and, after a reset with the default bound,
+    the job itself run as before."""
+    eng = Engine(0)
+    spec = W.slab2d(steps=256)
+    ref = eng.submit(spec, variant="tile", precision=np.float64)
+    ref.advance(128).sync()
+    want = {f: ref.field(f) for f in ("EZ", "HY")}
+    ref.release()
+
+    job = eng.submit(spec, variant="tile", precision=np.float64)
+    job.set_wait_limit(1)
+    job.advance(128)
+    with pytest.raises(TimeoutError_, match="bounded wait"):
+        job.sync(60000)
+    other = eng.submit(spec, variant="tile", precision=np.float64)  # the context still works
+    other.advance(128).sync(60000)
+    for f, v in want.items():
+        np.testing.assert_array_equal(other.field(f), v)
+    other.release()
+    job.set_wait_limit(0).reset().advance(128).sync(60000)  # default bound: the job recovers
+    for f, v in want.items():
+        np.testing.assert_array_equal(job.field(f), v)
+    job.release()
+    eng.close()

@@ -41,9 +41,10 @@ def _fixture_cases():
 
 
 def _case_variants():
-    """3D runs under every launch form (plane sweep, per-cell, vector, ordered); 2D has one."""
+    """3D runs under every launch form (plane sweep, per-cell, vector, ordered); 2D under both of its
+    forms (per-cell, tiles)."""
     return [(c, v) for c in _fixture_cases()
-            for v in (("sweep", "cell", "vec", "wave") if c.startswith("yee3d") else ("cell",))]
+            for v in (("sweep", "cell", "vec", "wave") if c.startswith("yee3d") else ("cell", "tile"))]
 
 
 @pytest.mark.parametrize("case,variant", _case_variants())
@@ -91,6 +92,10 @@ def _random_cases():
                                       core_x_nm=100, core_y_nm=120, seed=8),
         "yee3d_p2": lambda: W.strip3d(nx=17, ny=18, nz=35, P=2, src_gap=2, port_gap=4, steps=40, nf=3,
                                       core_x_nm=100, core_y_nm=140, source="TM", seed=9),
+        # the 2D tile form's shapes: a grid narrower than a halo, and rows longer than a
+        # block's threads
+        "tm2_narrow": lambda: W.slab2d(nx=14, ny=40, P=2, core_cells=7, src_x=4, ports=(6, 10), steps=40, nf=3),
+        "tm2_tall": lambda: W.slab2d(nx=37, ny=1100, P=3, core_cells=9, src_x=6, ports=(10, 28), steps=40, nf=3),
         "tm2_p1": lambda: W.slab2d(nx=40, ny=31, P=1, core_cells=7, src_x=6, ports=(10, 30), steps=40, nf=4,
                                    rough=True, sigma_nm=30, lc_nm=60, seed=4),
         # dt/eps coefficient grids perturbed cell by cell (thousands of distinct (x, y, z) triples),
@@ -129,16 +134,21 @@ def _te2_spec():
                                   "yee3d_p2", "yee3d_p2_cell", "tm2_p1", "yee3d_graded", "yee3d_graded_cell",
                                   "yee3d_te_vec", "yee3d_tm_vec", "yee3d_wide_vec", "yee3d_p1_vec", "yee3d_p2_vec",
                                   "yee3d_graded_vec", "yee3d_te_wave", "yee3d_tm_wave", "yee3d_wide_wave",
-                                  "yee3d_p1_wave", "yee3d_p2_wave", "yee3d_graded_wave"])
+                                  "yee3d_p1_wave", "yee3d_p2_wave", "yee3d_graded_wave", "tm2_tile",
+                                  "te2_tile", "tm2_p1_tile", "tm2_narrow_tile", "tm2_tall_tile",
+                                  "tm2_narrow", "tm2_tall", "tm2_tile2", "te2_tile2", "tm2_p1_tile2"])
 @pytest.mark.parametrize("ring", [1, 7, 32])
 def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     base, _, suffix = name.rpartition("_")
-    variant = {"cell": "cell", "vec": "vec", "wave": "wave"}.get(suffix, "sweep")
-    base = base if suffix in ("cell", "vec", "wave") else name
+    variant = suffix if suffix in ("cell", "vec", "wave", "tile", "tile2") else None
+    base = base if variant else name
+    variant = variant or ("sweep" if base.startswith("yee3d") else "cell")
+    # tile2: two steps per sub-block, so a ring block is a cooperative launch of many sub-blocks
+    choice = dict(variant="tile", tile_steps=2) if variant == "tile2" else dict(variant=variant)
     spec = _te2_spec() if base == "te2" else _random_cases()[base]()
     rng = np.random.default_rng(sum(map(ord, name)) + ring)
     s = oracle_from_spec(spec)
-    job = eng.submit(spec, arith="exact", precision=np.float64, ring_steps=ring, variant=variant)
+    job = eng.submit(spec, arith="exact", precision=np.float64, ring_steps=ring, **choice)
     for f in R.field_names(spec.mode):
         v = rng.standard_normal(spec.shape) * 1e-2
         getattr(s, f)[...] = v
@@ -200,7 +210,8 @@ def _field_errors(job, s, names):
                 float(np.linalg.norm(getattr(s, f).ravel()))) for f in names}
 
 
-def test_fp32_slab2d_full_run_within_targets(eng):
+@pytest.mark.parametrize("variant", ["tile", "cell"])
+def test_fp32_slab2d_full_run_within_targets(eng, variant):
     """The 400 x 200, 2000-step 2D case: float32 engine vs float64 oracle.
 
     Field error is checked at checkpoints while the pulse is in the domain
@@ -214,7 +225,7 @@ def test_fp32_slab2d_full_run_within_targets(eng):
     from oracle import cpu as OC
     from tests.helpers import dft_dict_oracle
     spec = W.slab2d()
-    job = eng.submit(spec, arith="fast", precision=np.float32)
+    job = eng.submit(spec, arith="fast", precision=np.float32, variant=variant)
     s = oracle_from_spec(spec)
     peak = {f: 0.0 for f in ("EZ", "HX", "HY")}
     prev = 0
@@ -268,13 +279,13 @@ def test_fp32_strip3d_within_targets(eng, variant):
 
 
 def test_batch_equals_single_jobs(eng):
-    """One multi-job advance over jobs of different solvers and sizes (2D TM,
-    2D TE, 3D sweep, 3D per-cell, 3D vector and ordered forms) equals advancing each job
-    alone, bit for bit (float64 EXACT), including an odd tail that flips
-    sweep buffers."""
+    """One multi-job advance over jobs of different solvers and sizes (2D TM
+    and TE in both 2D forms, 3D sweep, 3D per-cell, 3D vector and ordered
+    forms) equals advancing each job alone, bit for bit (float64 EXACT),
+    including an odd tail that flips sweep buffers."""
     specs = [_random_cases()["tm2"](), _te2_spec(), _random_cases()["yee3d_te"](), _random_cases()["yee3d_tm"](),
-             _random_cases()["yee3d_wide"](), _random_cases()["yee3d_p2"]()]
-    variants = ["cell", "cell", "sweep", "cell", "vec", "wave"]
+             _random_cases()["yee3d_wide"](), _random_cases()["yee3d_p2"](), _random_cases()["tm2"](), _te2_spec()]
+    variants = ["cell", "cell", "sweep", "cell", "vec", "wave", "tile", "tile"]
     solo, mix = [], []
     for sp, v in zip(specs, variants):
         solo.append(eng.submit(sp, arith="exact", precision=np.float64, ring_steps=6, variant=v))

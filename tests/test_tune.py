@@ -51,11 +51,25 @@ def test_descriptor_launch_choices_validated_on_host():
         d, keep = to_desc(spec, variant="vec", **bad)
         assert _bytes(lib, d)[0] == -1, bad
     slab = W.slab2d(nx=60, ny=50, P=5, core_cells=6, src_x=10, ports=(15, 45), steps=10, nf=3)
-    d, keep = to_desc(slab, rows=2)  # 2D has one launch form
+    d, keep = to_desc(slab, rows=2)  # tile rows belong to the 3D per-cell form
     assert _bytes(lib, d)[0] == -1
-    d, keep = to_desc(slab)
-    d.reserved[0] = 4  # no such launch form
+    for v in ("cell", "tile"):  # the 2D forms
+        d, keep = to_desc(slab, variant=v)
+        assert _bytes(lib, d)[0] == 0, v
+    for r0 in (1, 2, 3, 5):  # 3D forms, and no such form
+        d, keep = to_desc(slab)
+        d.reserved[0] = r0
+        assert _bytes(lib, d)[0] == -1, r0
+    d, keep = to_desc(spec, variant="tile")  # the tile form is 2D only
     assert _bytes(lib, d)[0] == -1
+    for steps in (1, 4, 8, 100):  # steps per launch (clamped to 8 and the ring)
+        d, keep = to_desc(slab, variant="tile", tile_steps=steps)
+        assert _bytes(lib, d)[0] == 0, steps
+    d, keep = to_desc(slab, variant="tile", tile_steps=-1)
+    assert _bytes(lib, d)[0] == -1
+    d, keep = to_desc(slab, variant="cell", tile_steps=4)  # steps per launch belong to the tile form
+    assert _bytes(lib, d)[0] == -1
+    assert to_desc(slab)[0].reserved[0] == 4  # 'auto': tiles in 2D
 
 
 class _FakeTuner(tune.Tuner):
@@ -89,7 +103,7 @@ def test_tuner_picks_fastest_and_caches_per_shape(tmp_path):
     t.choose(a, np.float64)  # precision is part of the key
     assert len(t.calls) == 3 * len(tune.CANDIDATES)
     slab = W.slab2d(nx=60, ny=50, P=5, core_cells=6, src_x=10, ports=(15, 45), steps=10, nf=3)
-    assert t.choose(slab) == tune.DEFAULT and len(t.calls) == 3 * len(tune.CANDIDATES)
+    assert t.choose(slab) == dict(tune.DEFAULT, variant="auto") and len(t.calls) == 3 * len(tune.CANDIDATES)
     saved = json.load(open(path))
     assert len(saved) == 3
     # a new tuner reads the file and measures nothing for known shapes
