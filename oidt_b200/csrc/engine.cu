@@ -509,7 +509,7 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
     return bad("reserved[0]: 2D launch form 0 (per-cell) or 4 (tiles)");
   if (d->reserved[1] != 0 && d->reserved[1] != 1) return bad("reserved[1]: 0 or 1");
   const int variant = d->reserved[0];
-  if (variant == kVariantTile && tile2d_smem(d->precision == OIDT_F32 ? 4 : 8, P) > kTileSmemMax)
+  if (variant == kVariantTile && tile2d_smem(d->precision == OIDT_F32 ? 4 : 8, P, kTileThreads, kTileThreads) > kTileSmemMax)
     return bad("tile form: num_cpml too large for a block's shared memory");
   if (variant == kVariantTile && ((long long)d->nx * d->ny > 0x7fffffffLL || (long long)d->nx * P > 0x7fffffffLL))
     return bad("tile form: the grid holds 2^31 or more cells");
@@ -740,7 +740,7 @@ template <typename T> void fill_params(Job *J) {
     p.ch = reinterpret_cast<const T *>(m + pl.off_ch);
     p.db = (T)d.db;
     p.dx = (T)d.dx;
-    p.rdx = (T)(1.0 / (double)p.dx);
+    p.rdx = T(1) / p.dx;  // RN(1/dx) in T (EXACT divisions by dx rely on it)
     p.psx = p.psy = pl.psi_pitch;
     p.wait_cycles = J->wait_cycles;
     for (auto fa : psi_pairs(d.mode))
@@ -836,7 +836,7 @@ template <typename T> int upload(oidt_ctx *ctx, Job *J, const oidt_job_desc *src
     const T *kd = static_cast<const T *>(d.kdx[a]);
     CU(ctx, cudaMemcpyAsync(m + pl.off_kd[a], kd, n * sizeof(T), cudaMemcpyHostToDevice, st));
     rk.resize(n);
-    for (int i = 0; i < n; ++i) rk[i] = (T)1 / kd[i];
+    for (int i = 0; i < n; ++i) rk[i] = (T)1 / kd[i];  // RN(1/kd) in T (EXACT divisions rely on it)
     CU(ctx, cudaMemcpyAsync(m + pl.off_rkd[a], rk.data(), n * sizeof(T), cudaMemcpyHostToDevice, st));
     CU(ctx, cudaStreamSynchronize(st));  // rk is reused
   }
@@ -1553,7 +1553,7 @@ int32_t oidt_job_create(oidt_ctx *ctx, const oidt_job_desc *desc, uint64_t *job)
   J->pl = pl;
   if (pl.variant == kVariantTile) {
     tile_plan(J, ctx->sms);
-    J->tile_smem = tile2d_smem(pl.esz, desc->num_cpml);
+    J->tile_smem = tile2d_smem(pl.esz, desc->num_cpml, J->tile.ti + 2 * J->tile.halo, J->tile.tj + 2 * J->tile.halo);
     // a ring block in one launch where every tile is resident at once and a tile's
     // halo reaches its 8 neighbours only
     J->tile_coop = ctx->coop && J->tile_blocks <= std::min(ctx->sms, kTileMaxBlocks) &&

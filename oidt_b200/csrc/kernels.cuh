@@ -26,12 +26,30 @@ enum { LO = 0, HI = 1 };
 // ---------------------------------------------------------------------------
 // Arithmetic policy.
 // ---------------------------------------------------------------------------
+// EXACT division a / b rounded to nearest, from y = RN(1/b) (the correctly
+// rounded reciprocal, computed on the host in the same precision) by two FMA
+// corrections: q1 = RN(q0 + r0 y), q2 = RN(q1 + r1 y) with q0 = RN(a y) and
+// the exact residuals r = a - b q.  q1 is within one ulp of a / b, so q2 is
+// the correctly rounded quotient by Markstein's theorem (P. Markstein, IBM J.
+// Res. Dev. 34(1), 1990; J.-M. Muller et al., Handbook of Floating-Point
+// Arithmetic, the division chapter), provided nothing under- or overflows:
+// the numerator, the quotient and the reciprocal stay within [2^-lo, 2^lo]
+// (the residuals are then exact); outside that range, and for NaN, the
+// quotient is divided directly.  Zero numerators give a zero of either sign.
 template <typename T, bool EXACT> struct Ar;
 template <> struct Ar<float, true> {
   static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
   static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
   static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
-  static __device__ __forceinline__ float div(float a, float b, float) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b, float y) {
+    const float q0 = __fmul_rn(a, y);
+    const float aa = fabsf(a), aq = fabsf(q0), ay = fabsf(y);
+    const bool ok = (a == 0.0f || (aa >= 0x1p-100f && aa <= 0x1p+100f && aq >= 0x1p-100f && aq <= 0x1p+100f)) &&
+                    ay >= 0x1p-100f && ay <= 0x1p+100f;
+    if (!ok) return __fdiv_rn(a, b);
+    const float q1 = __fmaf_rn(__fmaf_rn(-b, q0, a), y, q0);
+    return __fmaf_rn(__fmaf_rn(-b, q1, a), y, q1);
+  }
 };
 template <> struct Ar<float, false> {
   static __device__ __forceinline__ float add(float a, float b) { return a + b; }
@@ -43,7 +61,15 @@ template <> struct Ar<double, true> {
   static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
   static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
   static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-  static __device__ __forceinline__ double div(double a, double b, double) { return __ddiv_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b, double y) {
+    const double q0 = __dmul_rn(a, y);
+    const double aa = fabs(a), aq = fabs(q0), ay = fabs(y);
+    const bool ok = (a == 0.0 || (aa >= 0x1p-900 && aa <= 0x1p+900 && aq >= 0x1p-900 && aq <= 0x1p+900)) &&
+                    ay >= 0x1p-900 && ay <= 0x1p+900;
+    if (!ok) return __ddiv_rn(a, b);
+    const double q1 = __fma_rn(__fma_rn(-b, q0, a), y, q0);
+    return __fma_rn(__fma_rn(-b, q1, a), y, q1);
+  }
 };
 template <> struct Ar<double, false> {
   static __device__ __forceinline__ double add(double a, double b) { return a + b; }

@@ -12,12 +12,14 @@
 //   inside the held tile's edges (and up to the grid's edges, where there is
 //   nothing to read): after cnt <= halo steps the owned cells are exact.
 // * A held tile has at most kTileThreads cells, one per thread.  A thread
-//   works out its cell's update conditions, CPML slab coefficients, dt/eps
-//   and kappa values once per launch and keeps them in registers, and so
-//   its cell's three field values and CPML psi values through a sub-block of
-//   up to `halo` steps.  Shared memory holds the tile's fields only for the
+//   works out its cell's update conditions, CPML slab coefficients and dt/eps
+//   values once per launch and keeps them in registers, and so its cell's
+//   three field values and CPML psi values through a sub-block of up to
+//   `halo` steps.  Shared memory holds the tile's fields only for the
 //   neighbours' reads (each value written once per half-step by its cell's
-//   thread); __syncthreads separates the half-steps.
+//   thread), the CPML coefficient tables, and the kappa dx divisors with
+//   their reciprocals for the tile's rows and columns; __syncthreads
+//   separates the half-steps.
 // * Fields and psi are double-buffered: sub-block b reads the state of
 //   buffer par ^ (b & 1) and writes its owned cells to the other, so blocks
 //   loading halo cells never see cells another block has already advanced.
@@ -54,9 +56,13 @@ struct TileArgs {
   int *epoch;  // per tile: sub-blocks completed (cooperative launches)
 };
 
-// Shared memory of a block: the tile's three fields (kTileThreads cells each)
-// and the CPML coefficient tables be, ce, bh, ch (P each).
-inline size_t tile2d_smem(int esz, int P) { return (3 * (size_t)kTileThreads + 4 * (size_t)P) * esz; }
+// Shared memory of a block: the tile's three fields (kTileThreads cells each),
+// the CPML coefficient tables be, ce, bh, ch (P each), and per held row (at
+// most rows) kd0, 1/kd0, kd3, 1/kd3, per held column (at most cols) kd1,
+// 1/kd1, kd4, 1/kd4 (the kappa dx arrays: E x, H x, E y, H y).
+inline size_t tile2d_smem(int esz, int P, int rows, int cols) {
+  return (3 * (size_t)kTileThreads + 4 * (size_t)P + 4 * (size_t)rows + 4 * (size_t)cols) * esz;
+}
 
 // Cell flags.  TM: E1 = Ez update, H1 = Hx, H2 = Hy; TE: E1 = Ex, E2 = Ey,
 // H1 = Hz.  XE / YE / XH / YH: the cell is in the E / H x- / y-slab of the
@@ -78,6 +84,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T *const F0 = reinterpret_cast<T *>(smem_raw), *const F1 = F0 + kTileThreads, *const F2 = F1 + kTileThreads;
   T *const BE = F2 + kTileThreads, *const CE = BE + p.P, *const BH = CE + p.P, *const CH = BH + p.P;
+  T *const KR = CH + p.P, *const KC = KR + 4 * (a.ti + 2 * a.halo);  // kd / 1/kd by held row, column
   const int nx = p.nx, ny = p.ny, P = p.P, H = a.halo;
   const int bi = (int)blockIdx.x / a.gj, bj = (int)blockIdx.x - bi * a.gj;
   const int oi0 = bi * a.ti, oi1 = min(nx, oi0 + a.ti), oj0 = bj * a.tj, oj1 = min(ny, oj0 + a.tj);
@@ -90,7 +97,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
   // ---- the cell's constants ------------------------------------------------------------
   unsigned fl = 0;
   int qE = 0, qH = 0;  // slab coefficient indices + 1: x slab in bits 0-15, y slab in bits 16-31
-  T cbA = T(0), cbB = T(0), kEi = T(0), kEj = T(0), kHi = T(0), kHj = T(0);  // kd (EXACT) or 1/kd
+  T cbA = T(0), cbB = T(0);  // dt/eps of the cell's E components
   int capE[2] = {0, 0}, capH[2] = {0, 0};  // ring offsets of the cell's captures within a slot, per port
   // psi offsets of the cell in its slab arrays (x slab [P][ny], y slab [nx][P]) and their sides
   int oxE = 0, oyE = 0, oxH = 0, oyH = 0, sides = 0;  // sides: bit 0 x E, 1 y E, 2 x H, 3 y H
@@ -125,11 +132,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
     const bool up = li + 1 < nrow, right = lj + 1 < ncol, down = li > 0, left = lj > 0;
     const bool own = i >= oi0 && i < oi1 && j >= oj0 && j < oj1;
     if (own) fl |= kOwn;
-    auto K = [&](int a_, int x) { return EXACT ? __ldg(p.kd[a_] + x) : __ldg(p.rkd[a_] + x); };
-    kEi = K(0, i);
-    kEj = K(1, j);
-    kHi = K(3, i);
-    kHj = K(4, j);
     if (TM) {
       if (i >= p.ib && i < p.ie && j >= p.jb && j < p.je && up && right) fl |= kE1;   // update_ez :44-49
       if (i >= p.ib && i < p.ie && j > p.jb && j < p.je && left) fl |= kH1;          // update_hx :53-58
@@ -161,6 +163,14 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
     const T *src = u < P ? p.be : u < 2 * P ? p.ce : u < 3 * P ? p.bh : p.ch;
     BE[u] = __ldg(src + u % P);
   }
+  for (int u = t; u < 4 * (nrow + ncol); u += kTileThreads) {  // kappa dx and reciprocals, rows then columns
+    const int r = u >> 2, c = u & 3, a_ = r < nrow ? (c < 2 ? 0 : 3) : (c < 2 ? 1 : 4);
+    const int x = r < nrow ? wi0 + r : wj0 + (r - nrow);
+    const T v = __ldg((c & 1 ? p.rkd[a_] : p.kd[a_]) + x);
+    if (r < nrow) KR[u] = v;
+    else KC[u - 4 * nrow] = v;
+  }
+  const T *const kr = KR + 4 * li, *const kc = KC + 4 * lj;  // kd0 1/kd0 kd3 1/kd3 | kd1 1/kd1 kd4 1/kd4
   const T db = p.db;
   const long long cstride = 2LL * p.nslot * p.plane;  // ring slot pitch
   const int nsub = (a.cnt + H - 1) / H;
@@ -212,7 +222,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         if (fl & kE1) {  // update_ez :44-49
           const T dhy = A::sub(F2[t + ncol], f2);
           const T dhx = A::sub(F1[t + 1], f1);
-          T e = A::add(f0, A::mul(cbA, A::sub(A::div(dhy, kEi, kEi), A::div(dhx, kEj, kEj))));
+          T e = A::add(f0, A::mul(cbA, A::sub(A::div(dhy, kr[0], kr[1]), A::div(dhx, kc[0], kc[1]))));
           if (fl & kSrc) e = A::sub(e, __ldg(p.jsrc + n0 + s));  // update_source :71-76
           if (fl & kXE) {                                        // update_pml_ez_xinc :80-88
             const int q = (qE & 0xffff) - 1;
@@ -232,7 +242,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
       } else {
         if (fl & kE1) {  // update_ex :43-49
           const T dhz = A::sub(F2[t + 1], f2);
-          T e = A::add(f0, A::div(A::mul(cbA, dhz), kEj, kEj));
+          T e = A::add(f0, A::div(A::mul(cbA, dhz), kc[0], kc[1]));
           if (fl & kYE) {                                        // update_pml_ex_yinc :79-87
             const int q = (qE >> 16) - 1;
             ye = A::add(A::mul(BE[q], ye), A::div(A::mul(CE[q], dhz), p.dx, p.rdx));
@@ -243,7 +253,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         }
         if (fl & kE2) {  // update_ey :52-58
           const T hz1 = F2[t + ncol];
-          T e = A::add(f1, A::div(A::mul(cbB, A::sub(f2, hz1)), kEi, kEi));
+          T e = A::add(f1, A::div(A::mul(cbB, A::sub(f2, hz1)), kr[0], kr[1]));
           if (fl & kXE) {                                        // update_pml_ey_xinc :91-99
             const int q = (qE & 0xffff) - 1;
             xe = A::add(A::mul(BE[q], xe), A::div(A::mul(CE[q], A::sub(hz1, f2)), p.dx, p.rdx));
@@ -260,7 +270,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
       if (TM) {
         if (fl & kH1) {  // update_hx :53-58
           const T ezm = F0[t - 1];
-          T h = A::add(f1, A::div(A::mul(db, A::sub(ezm, f0)), kHj, kHj));
+          T h = A::add(f1, A::div(A::mul(db, A::sub(ezm, f0)), kc[2], kc[3]));
           if (fl & kYH) {                                        // update_pml_hx_yinc :104-112
             const int q = (qH >> 16) - 1;
             yh = A::add(A::mul(BH[q], yh), A::div(A::mul(CH[q], A::sub(f0, ezm)), p.dx, p.rdx));
@@ -271,7 +281,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         }
         if (fl & kH2) {  // update_hy :62-67
           const T dez = A::sub(f0, F0[t - ncol]);
-          T h = A::add(f2, A::div(A::mul(db, dez), kHi, kHi));
+          T h = A::add(f2, A::div(A::mul(db, dez), kr[2], kr[3]));
           if (fl & kXH) {                                        // update_pml_hy_xinc :116-124
             const int q = (qH & 0xffff) - 1;
             xh = A::add(A::mul(BH[q], xh), A::div(A::mul(CH[q], dez), p.dx, p.rdx));
@@ -286,7 +296,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         if (fl & kH1) {  // update_hz :61-67
           const T dex = A::sub(f0, F0[t - 1]);
           const T dey = A::sub(f1, F1[t - ncol]);
-          T h = A::add(f2, A::mul(db, A::sub(A::div(dex, kHj, kHj), A::div(dey, kHi, kHi))));
+          T h = A::add(f2, A::mul(db, A::sub(A::div(dex, kc[2], kc[3]), A::div(dey, kr[2], kr[3]))));
           if (fl & kSrc) h = A::sub(h, __ldg(p.jsrc + n0 + s));  // source after update_hz
           if (fl & kXH) {                                        // update_pml_hz_xinc :103-111
             const int q = (qH & 0xffff) - 1;
