@@ -513,10 +513,10 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
     return bad("tile form: num_cpml too large for a block's shared memory");
   if (variant == kVariantTile && ((long long)d->nx * d->ny > 0x7fffffffLL || (long long)d->nx * P > 0x7fffffffLL))
     return bad("tile form: the grid holds 2^31 or more cells");
-  const int rows = d->reserved[2] == 0 ? kRowsDefault : d->reserved[2];
+  const int rows = d->reserved[2] == 0 || variant == kVariantTile ? kRowsDefault : d->reserved[2];
   if (rows != 2 && rows != 4 && rows != 8) return bad("reserved[2]: tile rows 0 (default), 2, 4 or 8");
-  if (d->reserved[2] != 0 && !(is3 && variant == kVariantCell))
-    return bad("reserved[2] (tile rows) applies to the 3D per-cell form");
+  if (d->reserved[2] != 0 && !(is3 && variant == kVariantCell) && !(variant == kVariantTile && d->reserved[2] == 1))
+    return bad("reserved[2]: the 3D per-cell form's tile rows, or 1 (one launch per sub-block) for the 2D tile form");
   if (d->reserved[3] < 0 || (d->reserved[3] != 0 && !(is3 ? variant == kVariantSweep : variant == kVariantTile)))
     return bad("reserved[3] is >= 0: the 3D plane sweep's march depth or the 2D tile form's steps per launch");
   const int esz = d->precision == OIDT_F32 ? 4 : 8;
@@ -1556,7 +1556,7 @@ int32_t oidt_job_create(oidt_ctx *ctx, const oidt_job_desc *desc, uint64_t *job)
     J->tile_smem = tile2d_smem(pl.esz, desc->num_cpml, J->tile.ti + 2 * J->tile.halo, J->tile.tj + 2 * J->tile.halo);
     // a ring block in one launch where every tile is resident at once and a tile's
     // halo reaches its 8 neighbours only
-    J->tile_coop = ctx->coop && J->tile_blocks <= std::min(ctx->sms, kTileMaxBlocks) &&
+    J->tile_coop = ctx->coop && desc->reserved[2] == 0 && J->tile_blocks <= std::min(ctx->sms, kTileMaxBlocks) &&
                    J->tile.halo <= std::min(J->tile.ti, J->tile.tj) && J->pl.K > J->tile.halo;
   }
   if (cudaMallocAsync(reinterpret_cast<void **>(&J->mem), pl.total, ctx->upload) != cudaSuccess) {

@@ -31,7 +31,10 @@
 //   it finished sub-block b - 1 -- its owned cells written, its reads of the
 //   buffer this block writes next done.  Halo width <= tile extent, so no
 //   other tile's cells are read.  The wait is bounded (p.wait_cycles); on
-//   expiry the block records state[1] = 3 and goes on.
+//   expiry the block records state[1] = 3 and goes on.  Between sub-blocks
+//   only what other tiles read crosses global memory: a tile stores its owned
+//   cells within `halo` of its edges and reloads its halo cells; the other
+//   owned cells stay in registers (and are stored after the last sub-block).
 //
 // Per cell the arithmetic is that of kernels.cuh's tm2_e_cell / tm2_h_cell /
 // te2_e_cell / te2_h_cell (the reference's fdtd_funcs.py of FDTD_2D_TM and
@@ -71,7 +74,7 @@ inline size_t tile2d_smem(int esz, int P, int rows, int cols) {
 // x = port + 1).
 enum : unsigned {
   kE1 = 1u, kE2 = 2u, kH1 = 4u, kH2 = 8u, kSrc = 16u, kXE = 32u, kYE = 64u, kXH = 128u, kYH = 256u,
-  kCE0 = 512u, kCE1 = 1024u, kCH0 = 2048u, kCH1 = 4096u, kOwn = 8192u
+  kCE0 = 512u, kCE1 = 1024u, kCH0 = 2048u, kCH1 = 4096u, kOwn = 8192u, kBand = 16384u
 };
 
 template <typename T, bool EXACT, int MODE>
@@ -84,7 +87,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T *const F0 = reinterpret_cast<T *>(smem_raw), *const F1 = F0 + kTileThreads, *const F2 = F1 + kTileThreads;
   T *const BE = F2 + kTileThreads, *const CE = BE + p.P, *const BH = CE + p.P, *const CH = BH + p.P;
-  T *const KR = CH + p.P, *const KC = KR + 4 * (a.ti + 2 * a.halo);  // kd / 1/kd by held row, column
+  // kd, 1/kd tables (one array each, consecutive columns in consecutive banks): rows kd0 1/kd0 kd3 1/kd3,
+  // columns kd1 1/kd1 kd4 1/kd4
+  const int RM = a.ti + 2 * a.halo, CM = a.tj + 2 * a.halo;
+  T *const KR = CH + p.P, *const KC = KR + 4 * RM;
   const int nx = p.nx, ny = p.ny, P = p.P, H = a.halo;
   const int bi = (int)blockIdx.x / a.gj, bj = (int)blockIdx.x - bi * a.gj;
   const int oi0 = bi * a.ti, oi1 = min(nx, oi0 + a.ti), oj0 = bj * a.tj, oj1 = min(ny, oj0 + a.tj);
@@ -101,6 +107,20 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
   int capE[2] = {0, 0}, capH[2] = {0, 0};  // ring offsets of the cell's captures within a slot, per port
   // psi offsets of the cell in its slab arrays (x slab [P][ny], y slab [nx][P]) and their sides
   int oxE = 0, oyE = 0, oxH = 0, oyH = 0, sides = 0;  // sides: bit 0 x E, 1 y E, 2 x H, 3 y H
+  // this thread's entries of the coefficient and kappa dx tables, loaded first so that
+  // their latency overlaps the cell's own loads (leftovers past kTileThreads below)
+  const int nk = 4 * (nrow + ncol);
+  auto co_src = [&](int u) { return __ldg((u < P ? p.be : u < 2 * P ? p.ce : u < 3 * P ? p.bh : p.ch) + u % P); };
+  auto k_src = [&](int u, int &dst) {  // rows kd0 1/kd0 kd3 1/kd3, then columns kd1 1/kd1 kd4 1/kd4
+    const bool row = u < 4 * nrow;
+    const int v = row ? u : u - 4 * nrow, n = row ? nrow : ncol, c = v / n, r = v - c * n;
+    const int a_ = row ? (c < 2 ? 0 : 3) : (c < 2 ? 1 : 4);
+    dst = row ? c * RM + r : 4 * RM + c * CM + r;
+    return __ldg((c & 1 ? p.rkd[a_] : p.kd[a_]) + (row ? wi0 : wj0) + r);
+  };
+  int kdst = 0;
+  const T vco = t < 4 * P ? co_src(t) : T(0);
+  const T vk = t < nk ? k_src(t, kdst) : T(0);
   if (act) {
     int d, side, q;
     if ((q = e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {
@@ -132,6 +152,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
     const bool up = li + 1 < nrow, right = lj + 1 < ncol, down = li > 0, left = lj > 0;
     const bool own = i >= oi0 && i < oi1 && j >= oj0 && j < oj1;
     if (own) fl |= kOwn;
+    if (own && (i - oi0 < H || oi1 - i <= H || j - oj0 < H || oj1 - j <= H)) fl |= kBand;  // read by neighbour tiles
     if (TM) {
       if (i >= p.ib && i < p.ie && j >= p.jb && j < p.je && up && right) fl |= kE1;   // update_ez :44-49
       if (i >= p.ib && i < p.ie && j > p.jb && j < p.je && left) fl |= kH1;          // update_hx :53-58
@@ -159,24 +180,21 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
       }
     }
   }
-  for (int u = t; u < 4 * P; u += kTileThreads) {  // the CPML coefficients, be ce bh ch
-    const T *src = u < P ? p.be : u < 2 * P ? p.ce : u < 3 * P ? p.bh : p.ch;
-    BE[u] = __ldg(src + u % P);
+  if (t < 4 * P) BE[t] = vco;  // the CPML coefficients be ce bh ch, and the kappa dx tables
+  if (t < nk) KR[kdst] = vk;
+  for (int u = t + kTileThreads; u < 4 * P; u += kTileThreads) BE[u] = co_src(u);
+  for (int u = t + kTileThreads; u < nk; u += kTileThreads) {
+    int dst;
+    const T x = k_src(u, dst);
+    KR[dst] = x;
   }
-  for (int u = t; u < 4 * (nrow + ncol); u += kTileThreads) {  // kappa dx and reciprocals, rows then columns
-    const int r = u >> 2, c = u & 3, a_ = r < nrow ? (c < 2 ? 0 : 3) : (c < 2 ? 1 : 4);
-    const int x = r < nrow ? wi0 + r : wj0 + (r - nrow);
-    const T v = __ldg((c & 1 ? p.rkd[a_] : p.kd[a_]) + x);
-    if (r < nrow) KR[u] = v;
-    else KC[u - 4 * nrow] = v;
-  }
-  const T *const kr = KR + 4 * li, *const kc = KC + 4 * lj;  // kd0 1/kd0 kd3 1/kd3 | kd1 1/kd1 kd4 1/kd4
+  const T *const kr = KR + li, *const kc = KC + lj;  // kr[0, RM, 2 RM, 3 RM]: kd0 1/kd0 kd3 1/kd3; kc likewise
   const T db = p.db;
   const long long cstride = 2LL * p.nslot * p.plane;  // ring slot pitch
   const int nsub = (a.cnt + H - 1) / H;
-  pdl_wait();  // the previous launch's state is complete from here on
+  pdl_wait();  // the previous launch's state is complete (and visible) from here on
   const int n0 = p.state[0] + a.s0;
-  const int e0 = nsub > 1 ? ld_acquire(a.epoch + blockIdx.x) : 0;
+  const int e0 = nsub > 1 ? a.epoch[blockIdx.x] : 0;  // equal for every tile at launch
   T f0 = T(0), f1 = T(0), f2 = T(0), xe = T(0), ye = T(0), xh = T(0), yh = T(0);  // the cell's values
   for (int sb = 0; sb < nsub; ++sb) {
     T **rf = (sb & 1) ? p.fn : p.f;  // buffers read and written in this sub-block
@@ -201,7 +219,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
       }
       __syncthreads();
     }
-    if (act) {  // the held tile of the buffer read (L2: other blocks wrote it)
+    if (act && (sb == 0 || !(fl & kOwn))) {  // the held tile of the buffer read (L2: other blocks wrote it)
       f0 = __ldcg(rf[FA] + g);
       f1 = __ldcg(rf[FB] + g);
       f2 = __ldcg(rf[FC] + g);
@@ -222,7 +240,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         if (fl & kE1) {  // update_ez :44-49
           const T dhy = A::sub(F2[t + ncol], f2);
           const T dhx = A::sub(F1[t + 1], f1);
-          T e = A::add(f0, A::mul(cbA, A::sub(A::div(dhy, kr[0], kr[1]), A::div(dhx, kc[0], kc[1]))));
+          T e = A::add(f0, A::mul(cbA, A::sub(A::div(dhy, kr[0], kr[RM]), A::div(dhx, kc[0], kc[CM]))));
           if (fl & kSrc) e = A::sub(e, __ldg(p.jsrc + n0 + s));  // update_source :71-76
           if (fl & kXE) {                                        // update_pml_ez_xinc :80-88
             const int q = (qE & 0xffff) - 1;
@@ -242,7 +260,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
       } else {
         if (fl & kE1) {  // update_ex :43-49
           const T dhz = A::sub(F2[t + 1], f2);
-          T e = A::add(f0, A::div(A::mul(cbA, dhz), kc[0], kc[1]));
+          T e = A::add(f0, A::div(A::mul(cbA, dhz), kc[0], kc[CM]));
           if (fl & kYE) {                                        // update_pml_ex_yinc :79-87
             const int q = (qE >> 16) - 1;
             ye = A::add(A::mul(BE[q], ye), A::div(A::mul(CE[q], dhz), p.dx, p.rdx));
@@ -253,7 +271,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         }
         if (fl & kE2) {  // update_ey :52-58
           const T hz1 = F2[t + ncol];
-          T e = A::add(f1, A::div(A::mul(cbB, A::sub(f2, hz1)), kr[0], kr[1]));
+          T e = A::add(f1, A::div(A::mul(cbB, A::sub(f2, hz1)), kr[0], kr[RM]));
           if (fl & kXE) {                                        // update_pml_ey_xinc :91-99
             const int q = (qE & 0xffff) - 1;
             xe = A::add(A::mul(BE[q], xe), A::div(A::mul(CE[q], A::sub(hz1, f2)), p.dx, p.rdx));
@@ -270,7 +288,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
       if (TM) {
         if (fl & kH1) {  // update_hx :53-58
           const T ezm = F0[t - 1];
-          T h = A::add(f1, A::div(A::mul(db, A::sub(ezm, f0)), kc[2], kc[3]));
+          T h = A::add(f1, A::div(A::mul(db, A::sub(ezm, f0)), kc[2 * CM], kc[3 * CM]));
           if (fl & kYH) {                                        // update_pml_hx_yinc :104-112
             const int q = (qH >> 16) - 1;
             yh = A::add(A::mul(BH[q], yh), A::div(A::mul(CH[q], A::sub(f0, ezm)), p.dx, p.rdx));
@@ -281,7 +299,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         }
         if (fl & kH2) {  // update_hy :62-67
           const T dez = A::sub(f0, F0[t - ncol]);
-          T h = A::add(f2, A::div(A::mul(db, dez), kr[2], kr[3]));
+          T h = A::add(f2, A::div(A::mul(db, dez), kr[2 * RM], kr[3 * RM]));
           if (fl & kXH) {                                        // update_pml_hy_xinc :116-124
             const int q = (qH & 0xffff) - 1;
             xh = A::add(A::mul(BH[q], xh), A::div(A::mul(CH[q], dez), p.dx, p.rdx));
@@ -296,7 +314,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
         if (fl & kH1) {  // update_hz :61-67
           const T dex = A::sub(f0, F0[t - 1]);
           const T dey = A::sub(f1, F1[t - ncol]);
-          T h = A::add(f2, A::mul(db, A::sub(A::div(dex, kc[2], kc[3]), A::div(dey, kr[2], kr[3]))));
+          T h = A::add(f2, A::mul(db, A::sub(A::div(dex, kc[2 * CM], kc[3 * CM]), A::div(dey, kr[2 * RM], kr[3 * RM]))));
           if (fl & kSrc) h = A::sub(h, __ldg(p.jsrc + n0 + s));  // source after update_hz
           if (fl & kXH) {                                        // update_pml_hz_xinc :103-111
             const int q = (qH & 0xffff) - 1;
@@ -316,8 +334,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_2d_tile(Params<T> p, TileAr
       }
       __syncthreads();
     }
-    // ---- owned cells to the buffer written ------------------------------------------------
-    if (fl & kOwn) {
+    // ---- owned cells to the buffer written (before the last sub-block: those other tiles read)
+    if ((fl & kOwn) && (sb == nsub - 1 || (fl & kBand))) {
       wf[FA][g] = f0;
       wf[FB][g] = f1;
       wf[FC][g] = f2;

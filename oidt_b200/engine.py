@@ -135,23 +135,24 @@ class Engine:
         return {k: getattr(s, k) for k, _ in Stats._fields_}
 
     def job_bytes(self, spec: SimSpec, precision=None, ring_steps=0, variant: str = "auto", march_depth: int = 0,
-                  material: bool = True, tile_steps: int = 0) -> int:
+                  material: bool = True, tile_steps: int = 0, tile_coop: bool = True) -> int:
         d, keep = to_desc(spec, precision=precision, ring_steps=ring_steps, variant=variant, march_depth=march_depth,
-                          material=material, tile_steps=tile_steps)
+                          material=material, tile_steps=tile_steps, tile_coop=tile_coop)
         b = C.c_uint64()
         self._check(self.lib.oidt_job_bytes(C.byref(d), C.byref(b)))
         return b.value
 
     def submit(self, spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0,
                variant: str = "auto", graphs: bool = True, rows: int = 0, march_depth: int = 0,
-               material: bool = True, tile_steps: int = 0) -> "Job":
+               material: bool = True, tile_steps: int = 0, tile_coop: bool = True) -> "Job":
         """Create a job (the H2D boundary).  ``variant``, ``rows``,
-        ``march_depth``, ``tile_steps`` and ``ring_steps`` choose how it is
+        ``march_depth``, ``tile_steps``, ``tile_coop`` and ``ring_steps`` choose how it is
         launched, never what it computes (``oidt_b200.tune`` picks them by
         measurement); ``material`` passes a 3D spec's material index instead
         of its three dt/eps grids (the same values)."""
         d, keep = to_desc(spec, arith=arith, precision=precision, ring_steps=ring_steps, variant=variant,
-                          graphs=graphs, rows=rows, march_depth=march_depth, material=material, tile_steps=tile_steps)
+                          graphs=graphs, rows=rows, march_depth=march_depth, material=material, tile_steps=tile_steps,
+                          tile_coop=tile_coop)
         jid = C.c_uint64()
         self._check(self.lib.oidt_job_create(self.ctx, C.byref(d), C.byref(jid)))
         del keep

@@ -109,22 +109,25 @@ def power_window(spec: SimSpec):
         return tuple(map(tuple, w)) if w else ((spec.win_lo[0], spec.win_hi[0]), (spec.win_lo[1], spec.win_hi[1]))
     return tuple(w) if w else (spec.win_lo[1], spec.win_hi[1])
 
+
 def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int = 0, variant: str = "auto",
-            graphs: bool = True, rows: int = 0, march_depth: int = 0, material: bool = True, tile_steps: int = 0):
+            graphs: bool = True, rows: int = 0, march_depth: int = 0, material: bool = True, tile_steps: int = 0,
+            tile_coop: bool = True):
     """Build the ABI descriptor; returns (desc, keepalive) -- the arrays in
     ``keepalive`` must outlive the ``oidt_job_create`` call.
 
-    ``variant``: 'auto' (default) picks 'vec' in 3D and 'tile' in 2D.  3D: 'vec' -- the E-half / H-half
-    launches with four cells per thread along z and 16-byte accesses;
-    'wave' -- the same code in one launch per step, E and H half-steps
-    ordered plane by plane; 'cell' -- the half-steps with one cell per
-    thread; 'sweep' -- one plane-sweep launch per step (E and H fused,
-    TMA-staged tiles).  2D: 'cell' -- the E-half / H-half launches with one
-    cell per thread; 'tile' -- up to 8 steps per launch, each block advancing
-    a tile of the grid (and a halo around it) in shared memory.
-    ``tile_steps`` (2D tile form): steps per launch, 1 to 8 (0 = the
-    engine's estimate).
-    ``graphs=False``
+    ``variant``: 'auto' (default) picks 'vec' in 3D and 'tile' in 2D.
+    3D: 'vec' -- the E-half / H-half launches with four cells per thread
+    along z and 16-byte accesses; 'wave' -- the same code in one launch per
+    step, E and H half-steps ordered plane by plane; 'cell' -- the
+    half-steps with one cell per thread; 'sweep' -- one plane-sweep launch
+    per step (E and H fused, TMA-staged tiles).  2D: 'cell' -- the E-half /
+    H-half launches with one cell per thread; 'tile' -- each block advances
+    a tile of the grid (and a halo around it) in shared memory through
+    sub-blocks of up to 8 steps.  ``tile_steps`` (2D tile form): steps per
+    sub-block, 1 to 8 (0 = the engine's estimate); ``tile_coop``: a ring
+    block in one cooperative launch where every tile fits on the device at
+    once (default), else one launch per sub-block.  ``graphs=False``
     launches every step directly instead of replaying K-step CUDA graphs.
     ``rows`` (3D per-cell form): tile rows of a block, 2, 4 or 8 (0 = 4);
     ``march_depth`` (3D plane sweep): x-planes per work item (0 = the
@@ -181,9 +184,12 @@ def to_desc(spec: SimSpec, arith: str = "fast", precision=None, ring_steps: int 
     tw = [arr(t, np.float64) for t in spec.twiddles]
     d.cos_e, d.sin_e, d.cos_h, d.sin_h = tw
     d.ring_steps = ring_steps
-    d.reserved[0] = VARIANTS[resolve_variant(spec, variant)]
+    v = resolve_variant(spec, variant)
+    d.reserved[0] = VARIANTS[v]
     d.reserved[1] = 0 if graphs else 1
     d.reserved[2] = int(rows)
+    if v == "tile" and not tile_coop:
+        d.reserved[2] = 1
     d.reserved[3] = int(march_depth) or int(tile_steps)
     probe = spec.meta.get("probe")  # (y, z) of a 3D line probe along x
     if probe is not None:

@@ -136,15 +136,18 @@ def _te2_spec():
                                   "yee3d_graded_vec", "yee3d_te_wave", "yee3d_tm_wave", "yee3d_wide_wave",
                                   "yee3d_p1_wave", "yee3d_p2_wave", "yee3d_graded_wave", "tm2_tile",
                                   "te2_tile", "tm2_p1_tile", "tm2_narrow_tile", "tm2_tall_tile",
-                                  "tm2_narrow", "tm2_tall", "tm2_tile2", "te2_tile2", "tm2_p1_tile2"])
+                                  "tm2_narrow", "tm2_tall", "tm2_tile2", "te2_tile2", "tm2_p1_tile2",
+                                  "tm2_tile1", "te2_tile1"])
 @pytest.mark.parametrize("ring", [1, 7, 32])
 def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     base, _, suffix = name.rpartition("_")
-    variant = suffix if suffix in ("cell", "vec", "wave", "tile", "tile2") else None
+    variant = suffix if suffix in ("cell", "vec", "wave", "tile", "tile2", "tile1") else None
     base = base if variant else name
     variant = variant or ("sweep" if base.startswith("yee3d") else "cell")
-    # tile2: two steps per sub-block, so a ring block is a cooperative launch of many sub-blocks
-    choice = dict(variant="tile", tile_steps=2) if variant == "tile2" else dict(variant=variant)
+    # tile2: two steps per sub-block, so a ring block is a cooperative launch of many sub-blocks;
+    # tile1: one launch per sub-block
+    choice = {"tile2": dict(variant="tile", tile_steps=2),
+              "tile1": dict(variant="tile", tile_coop=False)}.get(variant, dict(variant=variant))
     spec = _te2_spec() if base == "te2" else _random_cases()[base]()
     rng = np.random.default_rng(sum(map(ord, name)) + ring)
     s = oracle_from_spec(spec)

@@ -69,6 +69,10 @@ def test_descriptor_launch_choices_validated_on_host():
     assert _bytes(lib, d)[0] == -1
     d, keep = to_desc(slab, variant="cell", tile_steps=4)  # steps per launch belong to the tile form
     assert _bytes(lib, d)[0] == -1
+    d, keep = to_desc(slab, variant="tile", tile_coop=False)  # one launch per sub-block: reserved[2] = 1
+    assert d.reserved[2] == 1 and _bytes(lib, d)[0] == 0
+    d.reserved[2] = 2  # nothing else
+    assert _bytes(lib, d)[0] == -1
     assert to_desc(slab)[0].reserved[0] == 4  # 'auto': tiles in 2D
 
 
