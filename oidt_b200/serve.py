@@ -90,7 +90,12 @@ class Result:
 class Server:
     def __init__(self, engine: Engine, tick: int = 64, precision=np.float32, arith: str = "fast",
                  keep_dfts: bool = False, ring_steps: int = 32, fair_share: bool = True, max_boost_log2: int = 6,
-                 small_cells: int = 1_000_000, max_large: int = 4):
+                 small_cells: int = 1_000_000, max_large: int = 4, variant_2d: str = "cell"):
+        """``variant_2d``: the launch form of 2D jobs.  The loop advances many
+        jobs at once, where the per-cell form (no halo recomputation, kernels
+        of different jobs running side by side) has the higher throughput;
+        the tile form, the engine's default for a job on its own, has the
+        lower latency for one job."""
         if tick % ring_steps:
             raise ValueError("tick must be a multiple of ring_steps")
         self.eng = engine
@@ -103,19 +108,22 @@ class Server:
         self.arith = arith
         self.keep_dfts = keep_dfts
         self.ring = ring_steps
+        self.variant_2d = variant_2d
         self.active = []   # (request, job, incident job or None, admit time)
         self.results = []
         self.refused = 0
 
     def _admit(self, req: Request, now: float) -> bool:
+        v = self.variant_2d if req.spec.mode != "yee3d" else "auto"
         try:
-            j = self.eng.submit(req.spec, arith=self.arith, precision=self.precision, ring_steps=self.ring)
+            j = self.eng.submit(req.spec, arith=self.arith, precision=self.precision, ring_steps=self.ring, variant=v)
         except BudgetError:
             return False
         ji = None
         if req.incident is not None:
             try:
-                ji = self.eng.submit(req.incident, arith=self.arith, precision=self.precision, ring_steps=self.ring)
+                ji = self.eng.submit(req.incident, arith=self.arith, precision=self.precision, ring_steps=self.ring,
+                                     variant=v)
             except BudgetError:
                 j.release()
                 return False
