@@ -31,11 +31,13 @@
 extern "C" {
 #endif
 
-#define OIDT_ABI_VERSION 4  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe);
+#define OIDT_ABI_VERSION 5  /* 2: line probe (oidt_job_desc.probe, oidt_job_read_probe);
                               3: launch choices (reserved[2..3]), oidt_job_port_power;
                               4: oidt_job_read_dft_window_static, the vector and ordered
                                  launch forms (reserved[0] = 2, 3), oidt_job_set_wait_limit,
-                                 the material index (mat_idx, mat_tab, nmat) */
+                                 the material index (mat_idx, mat_tab, nmat);
+                              5: the 2D tile form (reserved[0] = 4 in 2D, its choices in
+                                 reserved[2..3]); 2D jobs take launch forms 0 and 4 only */
 
 /* status codes */
 #define OIDT_OK 0
@@ -102,17 +104,24 @@ typedef struct oidt_job_desc {
   /* float64 twiddles [nf][nt]: cos/sin(2 pi f n dt) and at (n + 1/2) dt */
   const double *cos_e, *sin_e, *cos_h, *sin_h;
   int32_t ring_steps; /* steps buffered between DFT folds (0 = default)    */
-  /* reserved[0]: 3D launch form, 0 = per-cell E-half / H-half launches,
+  /* reserved[0]: launch form.  3D: 0 = per-cell E-half / H-half launches,
    *              1 = plane sweep (one launch per step),
    *              2 = vector form: the E-half / H-half launches with four
    *                  cells per thread along z and 16-byte accesses,
    *              3 = ordered form: the vector form's code in one launch per
-   *                  step, E and H half-steps ordered plane by plane;
+   *                  step, E and H half-steps ordered plane by plane.
+   *              2D: 0 = per-cell E-half / H-half launches,
+   *              4 = tile form: each block advances a tile of the grid and a
+   *                  halo around it through sub-blocks of up to 8 steps in
+   *                  shared memory; a ring block is one cooperative launch
+   *                  where every tile is resident at once;
    * reserved[1]: 1 = launch every step directly (no CUDA-graph replay);
-   * reserved[2]: 3D per-cell form only: rows of a block's 32 x rows tile,
-   *              2, 4 or 8 (0 = 4);
-   * reserved[3]: 3D plane sweep only: march depth, the x-planes of one work
-   *              item (0 = the engine's makespan estimate).
+   * reserved[2]: 3D per-cell form: rows of a block's 32 x rows tile,
+   *              2, 4 or 8 (0 = 4); 2D tile form: 1 = one launch per
+   *              sub-block instead of the cooperative launch;
+   * reserved[3]: 3D plane sweep: march depth, the x-planes of one work item
+   *              (0 = the engine's makespan estimate); 2D tile form: steps
+   *              per sub-block, 1 to 8 (0 = the engine's estimate).
    * None of these changes results; they are launch choices, measured per
    * grid shape by the host's tuner.  Other values are OIDT_ERR_INVALID. */
   int32_t reserved[4];
@@ -250,13 +259,16 @@ int32_t oidt_job_release(oidt_ctx *ctx, uint64_t job);
 int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job);
 
 /* Bound, in SM clock cycles, on each wait of the plane-sweep kernel
- * (reserved[0] = 1) for a plane's tile loads; cycles <= 0 restores the
- * default (4e9, about 2 s).  A wait that runs out marks the job failed --
- * oidt_job_sync then returns OIDT_ERR_TIMEOUT -- and the kernel returns after
- * the copies it has in flight have landed (those waits keep the default
- * bound).  For tests of that failure path: a small bound makes the waits run
- * out on loads that are merely in flight.  No counterpart in the reference
- * (its kernels do not wait on one another). */
+ * (reserved[0] = 1) for a plane's tile loads, and of the 2D tile form's
+ * cooperative launch for its neighbour tiles between sub-blocks; cycles <= 0
+ * restores the default (4e9, about 2 s).  A wait that runs out marks the job
+ * failed -- oidt_job_sync then returns OIDT_ERR_TIMEOUT -- and the kernel
+ * still ends: the plane sweep after the copies it has in flight have landed
+ * (those waits keep the default bound), the tile form's blocks without
+ * waiting again in that launch.  For tests of that failure path: a small
+ * bound makes the waits run out on loads or neighbours that are merely in
+ * flight.  No counterpart in the reference (its kernels do not wait on one
+ * another). */
 int32_t oidt_job_set_wait_limit(oidt_ctx *ctx, uint64_t job, int64_t cycles);
 
 /* The context's compute stream (a cudaStream_t), so callers can order their

@@ -17,7 +17,7 @@ from .spec import DFT_COMPS, FIELD_ID, FIELDS, PSI, SimSpec, to_desc
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboidt.so")
 
-ABI_VERSION = 4  # OIDT_ABI_VERSION of include/oidt.h
+ABI_VERSION = 5  # OIDT_ABI_VERSION of include/oidt.h
 OK, ERR_INVALID, ERR_CUDA, ERR_BUDGET, ERR_NOTFOUND, ERR_TIMEOUT, ERR_STATE = 0, -1, -2, -3, -4, -5, -6
 EXPORTS = ("oidt_abi_version", "oidt_create", "oidt_destroy", "oidt_last_error", "oidt_stats_get",
            "oidt_job_bytes", "oidt_job_create", "oidt_job_advance", "oidt_batch_advance", "oidt_job_sync",
