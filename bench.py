@@ -445,7 +445,12 @@ def run_engine(args, ws, rank, local):
                                                    "gbs": round(half["E"] / (ms_e * 1e-3) / 1e9, 1)},
                                         "k_v3_h": {"ms": round(ms_h, 5), "bytes": half["H"],
                                                    "gbs": round(half["H"] / (ms_h * 1e-3) / 1e9, 1)},
-                                        "k_fold_per_16_steps_ms": round(ms_fold, 5)}},
+                                        "k_fold_per_16_steps_ms": round(ms_fold, 5)},
+                         # the same graph-replayed step over the bytes its two launches move (each
+                         # half-step re-reads the fields the other writes), not the fused 60 B/cell
+                         "two_launch": {"bytes_per_step": int(half["E"] + half["H"]),
+                                        "achieved_gbs": round((half["E"] + half["H"]) / (ms_ts * 1e-3) / 1e9, 1),
+                                        "frac": round((half["E"] + half["H"]) / (ms_ts * 1e-3) / 1e9 / peak, 4)}},
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e, 3)},
