@@ -2,7 +2,8 @@
 //
 // A 2D job of the served sizes (a few hundred x a few hundred cells) is too
 // small to fill the GPU, so with one launch per half-step its step time is
-// launch latency.  Here one launch advances up to `halo` steps:
+// launch latency.  Here the grid advances in sub-blocks of up to `halo` steps,
+// a launch covering one sub-block or a whole ring block of them:
 //
 // * The grid is cut into tiles, one block each.  Block (bi, bj) owns the
 //   cells [oi0, oi1) x [oj0, oj1) and also computes `halo` cells on every side
@@ -48,7 +49,7 @@
 namespace oidt {
 
 constexpr int kTileThreads = 1024;  // also the most cells a held tile has
-constexpr int kTileHaloMax = 8;     // steps per launch at most
+constexpr int kTileHaloMax = 8;     // steps per sub-block at most
 
 struct TileArgs {
   int s0;      // ring slot of the launch's first step
