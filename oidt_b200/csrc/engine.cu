@@ -55,7 +55,7 @@ constexpr int kBlock2 = 128;
 constexpr int TY = kSweepTY, TZ = kSweepTZ, ST = kSweepStages;  // owned tile of a sweep CTA
 constexpr int EYB = kSweepEY, EZB = kSweepEZ;                      // its thread box
 constexpr int kVariantCell = 0, kVariantSweep = 1, kVariantVec = 2, kVariantWave = 3;  // oidt_job_desc.reserved[0]
-constexpr int kVariantTile = 4;  // 2D: tiles advanced up to kTileHaloMax steps per launch in shared memory
+constexpr int kVariantTile = 4;  // 2D: tiles advanced in sub-blocks of up to kTileHaloMax steps (tile2d.cuh)
 constexpr int kTileMaxBlocks = 1024;  // tiles of a cooperative (several sub-block) launch at most
 constexpr size_t kTileSmemMax = 227 * 1024;  // shared memory of a tile block at most
 
