@@ -309,6 +309,37 @@ def test_batch_equals_single_jobs(eng):
         j.release()
 
 
+def test_tile_form_in_waves_equals_per_cell(eng):
+    """A served-size 2D grid (800 x 300) has more tiles than the B200 has SMs,
+    so its sub-blocks run as separate launches in waves: fields, CPML psi and
+    DFTs equal the per-cell launches' bit for bit (float64 EXACT), at ring
+    sizes that end blocks mid-sub-block."""
+    from oidt_b200 import workloads as W
+    from oidt_b200.spec import PSI
+    spec = W.slab2d(nx=800, ny=300, P=10, core_cells=10, src_x=40, ports=(60, 740), steps=60, nf=5,
+                    rough=True, sigma_nm=10, lc_nm=50, seed=2)
+    rng = np.random.default_rng(5)
+    init = {f: rng.standard_normal(spec.shape) * 1e-2 for f in R.field_names("tm2")}
+    jobs = []
+    for variant in ("tile", "cell"):
+        j = eng.submit(spec, arith="exact", precision=np.float64, ring_steps=7, variant=variant)
+        for f, v in init.items():
+            j.set_field(f, v)
+        j.advance(30).sync(60000)
+        jobs.append(j)
+    a, b = jobs
+    for f in R.field_names("tm2"):
+        np.testing.assert_array_equal(a.field(f), b.field(f), err_msg=f)
+    for name, axis in PSI["tm2"]:
+        for side in (0, 1):
+            np.testing.assert_array_equal(a.psi(name, axis, side), b.psi(name, axis, side))
+    for port in (0, 1):
+        for c in range(2):
+            np.testing.assert_array_equal(a.dft(port, c), b.dft(port, c))
+    for j in jobs:
+        j.release()
+
+
 def test_reset_reruns_identically(eng):
     """oidt_job_reset returns a job to step 0: a second run equals the first."""
     spec = _random_cases()["yee3d_te"]()
