@@ -11,7 +11,8 @@
 * ``batch`` -- batched roughness realizations; ``serve`` -- the continuous-
   batching request loop; ``tune`` -- per-shape launch choices.
 * ``scatter``, ``zwave`` -- the scattering-loss and wave-impedance
-  workloads; ``large`` -- the 151 M-cell run; ``prof`` -- profiler cases.
+  workloads; ``large`` -- the 151 M-cell run (profiler cases are
+  ``bench.py --ncu-case``).
 * ``build`` -- compiles ``liboidt.so`` in-tree.
 
 Nothing here falls back to the CPU: without the library, ``engine`` raises.
