@@ -40,8 +40,11 @@ constexpr int kVecThreads = 128;
 // (measured: with six blocks C2 73.9 us and a 384 x 384 x 256 grid 0.612 ms
 // per step, against 83.6 and 0.694 with the compiler's own 96-107 registers).
 // FP64 values take two registers each: three blocks (170 registers) keep the
-// FP64 kernels from spilling.
+// FP64 kernels from spilling.  The E half-step runs seven blocks (72
+// registers, a few spills to L1): C2 71.6 against 72.8 us per step; eight
+// blocks (64 registers) spill more and lose (76.1).
 constexpr int kVecBlocksPerSM = 6;
+constexpr int kVecBlocksPerSME = 7;
 
 template <typename T> struct V4 { T v[4]; };
 
@@ -727,7 +730,7 @@ __device__ __forceinline__ void v3_h_block(const Params<T> &p, const VecGeom &g,
 }
 
 template <typename T, bool EXACT>
-__global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSM : 3) k_v3_e(Params<T> p, VecGeom g, int s) {
+__global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? kVecBlocksPerSME : 3) k_v3_e(Params<T> p, VecGeom g, int s) {
   pdl_wait();
   v3_e_block<T, EXACT>(p, g, p.ib + blockIdx.y, blockIdx.x, s);
 }
