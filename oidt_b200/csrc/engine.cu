@@ -331,13 +331,30 @@ std::vector<int> cb_of(int mode) {  // which cb slots are used
 
 // Elements of one psi slab array in the reference's shape; `pitch` is the
 // device row length along z of the x- and y-slab arrays (nz, or nzp for the
-// vector form's 16-byte rows).
-long long psi_elems(int mode, int axis, int nx, int ny, int nz, int P, int pitch = 0) {
+// vector form's 16-byte rows), `zpitch` that of the z-slab arrays (P, or the
+// vector form's padded rows).
+long long psi_elems(int mode, int axis, int nx, int ny, int nz, int P, int pitch = 0, int zpitch = 0) {
   if (mode != OIDT_MODE_YEE3D) return (long long)(axis == AX ? P * (long long)ny : (long long)nx * P);
   const long long row = pitch > 0 ? pitch : nz;
   if (axis == AX) return (long long)P * ny * row;
   if (axis == AY) return (long long)nx * P * row;
-  return (long long)nx * ny * P;
+  return (long long)nx * ny * (zpitch > 0 ? zpitch : P);
+}
+
+// The vector form's z-slab psi rows.  A row holds every four-cell group that
+// meets the slab: slab cell d of the low side (k = kb + d) sits at
+// zoff[LO] + d = k - floor4(kb), of the high side (k = ke - P + d) at
+// zoff[HI] + d = k - floor4(ke - P).  A group k0 of the slab's groups then
+// reads its four values at one 16-byte aligned offset, k0 - floor4(start).
+struct ZRows {
+  int pitch, off[2];
+};
+ZRows z_rows(int kb, int ke, int P) {
+  ZRows z;
+  z.off[0] = kb - kb / 4 * 4;
+  z.off[1] = (ke - P) - (ke - P) / 4 * 4;
+  z.pitch = (std::max(z.off[0], z.off[1]) + P + 3) / 4 * 4;
+  return z;
 }
 
 struct JobPlan {
@@ -355,6 +372,8 @@ struct JobPlan {
   int K, esz, nzp, nbuf, variant, L, nitems;
   int rows;  // 3D per-cell tile rows
   int psi_pitch;  // row length along z of the 3D x- and y-slab psi arrays (nz or nzp)
+  int psz;        // row length of the 3D z-slab psi arrays (P, or the vector form's padded rows) ...
+  int zoff[2];    // ... and the place of slab cell d = 0 in a row, per side
 };
 
 // Flags of the work item whose E box starts at (y0 - 1, z0 - 1) (rows
@@ -529,13 +548,14 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   const int nbuf = variant == kVariantSweep || variant == kVariantTile ? 2 : 1;
   const bool vec_rows = variant == kVariantVec || variant == kVariantWave;  // the vector form's kernels
   const int psi_pitch = vec_rows ? nzp : d->nz;
+  const ZRows zr = vec_rows ? z_rows(d->kb, d->ke, P) : ZRows{P, {0, 0}};
   if (variant == kVariantWave) {  // block counts per plane and step stay in 32-bit counters
     const long long nb = vec_blocks_per_plane(d, nzp);
     if ((long long)(d->nt + 1) * nb > 0x7fffffffLL) return bad("ordered form: nt x blocks per plane >= 2^31");
   }
   if (vec_rows) {  // 32-bit row offsets of the pitched slabs; x-planes on grid.y
     const long long lim = 0x7fffffffLL;
-    if ((long long)P * d->ny * nzp > lim || (long long)d->nx * P * nzp > lim)
+    if ((long long)P * d->ny * nzp > lim || (long long)d->nx * P * nzp > lim || (long long)d->nx * d->ny * zr.pitch > lim)
       return bad("grid too large: a pitched CPML slab holds 2^31 or more elements");
     if (d->ie - d->ib > 65535) return bad("vector form: at most 65535 updated x-planes");
   }
@@ -558,7 +578,8 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   for (auto fa : psi_pairs(d->mode))
     for (int b = 0; b < psi_bufs(nbuf, variant, fa.first); ++b)
       for (int sd = 0; sd < 2; ++sd)
-        pl->off_psi[b][fa.first][fa.second][sd] = L.take(psi_elems(d->mode, fa.second, d->nx, d->ny, d->nz, P, psi_pitch) * esz);
+        pl->off_psi[b][fa.first][fa.second][sd] =
+            L.take(psi_elems(d->mode, fa.second, d->nx, d->ny, d->nz, P, psi_pitch, zr.pitch) * esz);
   pl->off_jsrc = L.take((size_t)d->nt * esz);
   for (int t = 0; t < 4; ++t) pl->off_tw[t] = L.take((size_t)d->nf * d->nt * 8);
   pl->off_ring = L.take((size_t)K * 2 * nslot_of(d->mode) * plane * esz);
@@ -589,6 +610,9 @@ int plan_job(const oidt_job_desc *d, JobPlan *pl, std::string *why) {
   pl->K = K;
   pl->rows = rows;
   pl->psi_pitch = psi_pitch;
+  pl->psz = zr.pitch;
+  pl->zoff[0] = zr.off[0];
+  pl->zoff[1] = zr.off[1];
   pl->esz = esz;
   pl->nzp = nzp;
   pl->nbuf = nbuf;
@@ -742,11 +766,13 @@ template <typename T> void fill_params(Job *J) {
     p.dx = (T)d.dx;
     p.rdx = T(1) / p.dx;  // RN(1/dx) in T (EXACT divisions by dx rely on it)
     p.psx = p.psy = pl.psi_pitch;
+    p.psz = d.mode == OIDT_MODE_YEE3D ? pl.psz : d.num_cpml;
     p.wait_cycles = J->wait_cycles;
     for (auto fa : psi_pairs(d.mode))
       for (int sd = 0; sd < 2; ++sd) {
         const bool two = psi_bufs(pl.nbuf, pl.variant, fa.first) == 2;
-        p.psi[fa.first][fa.second][sd] = reinterpret_cast<T *>(m + pl.off_psi[two ? bb : 0][fa.first][fa.second][sd]);
+        p.psi[fa.first][fa.second][sd] = reinterpret_cast<T *>(m + pl.off_psi[two ? bb : 0][fa.first][fa.second][sd]) +
+                                         (fa.second == AZ ? pl.zoff[sd] : 0);
         p.psin[fa.first][fa.second][sd] = p.psi[fa.first][fa.second][sd];  // in place
       }
     p.src_field = d.src_field;
@@ -1951,9 +1977,14 @@ int32_t oidt_job_read_psi(oidt_ctx *ctx, uint64_t job, int32_t field, int32_t ax
   const int b = psi_bufs(J->pl.nbuf, J->pl.variant, field) == 2 ? J->parity : 0;
   const unsigned char *src = J->mem + J->pl.off_psi[b][field][axis][side];
   const bool pitched = J->d.mode == OIDT_MODE_YEE3D && axis != AZ && J->pl.psi_pitch != J->d.nz;
+  const bool zpitched = J->d.mode == OIDT_MODE_YEE3D && axis == AZ && J->pl.psz != J->d.num_cpml;
   if (pitched) {  // rows of nz cells out of rows of psi_pitch cells
     const size_t row = (size_t)J->d.nz * J->pl.esz, pitch = (size_t)J->pl.psi_pitch * J->pl.esz;
     CU(ctx, cudaMemcpy2D(out, row, src, pitch, row, need / row, cudaMemcpyDeviceToHost));
+  } else if (zpitched) {  // rows of P cells out of the padded rows, from the side's first slab cell
+    const size_t row = (size_t)J->d.num_cpml * J->pl.esz, pitch = (size_t)J->pl.psz * J->pl.esz;
+    CU(ctx, cudaMemcpy2D(out, row, src + (size_t)J->pl.zoff[side] * J->pl.esz, pitch, row, need / row,
+                         cudaMemcpyDeviceToHost));
   } else {
     CU(ctx, cudaMemcpy(out, src, need, cudaMemcpyDeviceToHost));
   }
@@ -1989,7 +2020,7 @@ int32_t oidt_job_reset(oidt_ctx *ctx, uint64_t job) {
       for (int sd = 0; sd < 2; ++sd)
         CU(ctx, cudaMemsetAsync(J->mem + pl.off_psi[b][fa.first][fa.second][sd], 0,
                                 psi_elems(J->d.mode, fa.second, J->d.nx, J->d.ny, J->d.nz, J->d.num_cpml,
-                                          pl.psi_pitch) * pl.esz, st));
+                                          pl.psi_pitch, pl.psz) * pl.esz, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_ring, 0, pl.off_acc - pl.off_ring, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_acc, 0, pl.off_state - pl.off_acc, st));
   CU(ctx, cudaMemsetAsync(J->mem + pl.off_state, 0, 64, st));

@@ -120,6 +120,9 @@ template <typename T> struct Params {
   T *psin[6][3][2];      // E psi written (== psi for the per-cell launches)
   int psx, psy;          // row pitch (elements along z) of the x- and y-slab psi arrays:
                          // nz (the reference layout) or nzp (16-byte rows, vector form)
+  int psz;               // row pitch of the z-slab psi arrays: P (the reference layout), or
+                         // the vector form's rows of whole four-cell groups (psi[f][AZ][side]
+                         // then points at slab cell d = 0 of row 0, inside the padded row)
   const void *tmap_f;    // plane sweep: 6 CUtensorMaps of f[] (device memory)
   const void *tmap_cb;   // plane sweep: 3 CUtensorMaps of cb[]
   long long wait_cycles; // plane sweep: bound on each wait for a plane's tile loads
@@ -140,12 +143,12 @@ __device__ __forceinline__ bool in_src(const Params<T> &p, int fld, int i, int j
 }
 
 // psi array index for a 3D slab array whose `axis` extent is P: x-slabs
-// [P][ny][psx], y-slabs [nx][P][psy], z-slabs [nx][ny][P].
+// [P][ny][psx], y-slabs [nx][P][psy], z-slabs [nx][ny][psz].
 template <typename T>
 __device__ __forceinline__ long long psi_idx3(const Params<T> &p, int axis, int i, int j, int k) {
   if (axis == AX) return ((long long)i * p.ny + j) * p.psx + k;  // i is the slab index d
   if (axis == AY) return ((long long)i * p.P + j) * p.psy + k;   // j is d
-  return ((long long)i * p.ny + j) * p.P + k;                    // k is d
+  return ((long long)i * p.ny + j) * p.psz + k;                  // k is d
 }
 
 // E-field CPML slab test along one axis: returns coefficient index or -1,
@@ -494,7 +497,7 @@ __device__ __forceinline__ void y3_e_masked(const Params<T> &p, int i, int j, in
     }
   }
   if (kc && (q = e_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_ex_zinc, update_pml_ey_zinc
-    const int oa = (i * p.ny + j) * P + d;
+    const int oa = (i * p.ny + j) * p.psz + d;
     if (mex) {
       T *const px = p.psi[EX][AZ][side] + oa;
       const T vx = A::add(A::mul(p.be[q], *px), A::div(A::mul(p.ce[q], dhy_z), p.dx, p.rdx));
@@ -577,7 +580,7 @@ __device__ __forceinline__ void y3_h_masked(const Params<T> &p, int i, int j, in
     }
   }
   if (ko && (q = h_slab(k, p.kb, p.ke, P, d, side)) >= 0) {  // update_pml_hx_zinc, update_pml_hy_zinc
-    const int oa = (i * p.ny + j) * P + d;
+    const int oa = (i * p.ny + j) * p.psz + d;
     if (mhx) {
       T *const px = p.psi[HX][AZ][side] + oa;
       const T vx = A::add(A::mul(p.bh[q], *px), A::div(A::mul(p.ch[q], dey_z), p.dx, p.rdx));

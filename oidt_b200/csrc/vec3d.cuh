@@ -244,32 +244,70 @@ __device__ __forceinline__ void v3_edge_e(const Params<T> &p, const VecGeom &g, 
     st4(px, Px.v);
     st4(pz, Pz.v);
   }
-  // update_pml_ex_zinc, update_pml_ey_zinc: every old z-slab psi value of the
-  // group is read before the first is written
-  int qz[4], dz[4], sz[4];
-  T zx[4], zy[4];
-  const long long ob = ((long long)i * p.ny + j) * P;  // z-slab psi row (i, j)
+  // update_pml_ex_zinc, update_pml_ey_zinc.  The z-slab psi rows are padded to whole four-cell
+  // groups: when the group's slab cells lie on one side (always unless
+  // ke - kb < 2P + 3), its four values are one 16-byte aligned vector of the
+  // row (the rim cells' elements are padding, written back as read);
+  // otherwise cell by cell.
+  int qz[4], dz[4], zside = -1;
+  bool zmix = false;
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
+    int sd = 0;
     dz[m] = 0;
-    sz[m] = 0;
-    qz[m] = mex[m] || mey[m] ? e_slab(k0 + m, p.kb, p.ke, P, dz[m], sz[m]) : -1;
-    zx[m] = qz[m] >= 0 && mex[m] ? p.psi[EX][AZ][sz[m]][ob + dz[m]] : T(0);
-    zy[m] = qz[m] >= 0 && mey[m] ? p.psi[EY][AZ][sz[m]][ob + dz[m]] : T(0);
-  }
-#pragma unroll
-  for (int m = 0; m < 4; ++m) {
-    if (qz[m] < 0) continue;
-    const T be = p.be[qz[m]], ce = p.ce[qz[m]];
-    if (mex[m]) {
-      zx[m] = A::add(A::mul(be, zx[m]), A::div(A::mul(ce, dyz[m]), p.dx, p.rdx));
-      p.psi[EX][AZ][sz[m]][ob + dz[m]] = zx[m];
-      e0[m] = A::sub(e0[m], A::mul(C0.v[m], zx[m]));
+    qz[m] = mex[m] || mey[m] ? e_slab(k0 + m, p.kb, p.ke, P, dz[m], sd) : -1;
+    if (qz[m] >= 0) {
+      zmix |= zside >= 0 && zside != sd;
+      zside = sd;
     }
-    if (mey[m]) {
-      zy[m] = A::add(A::mul(be, zy[m]), A::div(A::mul(ce, dxz[m]), p.dx, p.rdx));
-      p.psi[EY][AZ][sz[m]][ob + dz[m]] = zy[m];
-      e1[m] = A::add(e1[m], A::mul(C1.v[m], zy[m]));
+  }
+  const long long ob = ((long long)i * p.ny + j) * p.psz;  // z-slab psi row (i, j)
+  if (zside >= 0 && !zmix) {
+    const int off = k0 - (zside ? p.ke - P : p.kb);  // slab index d of the group's first cell
+    T *const qx = p.psi[EX][AZ][zside] + (ob + off), *const qy = p.psi[EY][AZ][zside] + (ob + off);
+    V4<T> Zx, Zy;
+    ldw4(Zx, qx);
+    ldw4(Zy, qy);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (qz[m] < 0) continue;
+      const T be = p.be[qz[m]], ce = p.ce[qz[m]];
+      if (mex[m]) {
+        Zx.v[m] = A::add(A::mul(be, Zx.v[m]), A::div(A::mul(ce, dyz[m]), p.dx, p.rdx));
+        e0[m] = A::sub(e0[m], A::mul(C0.v[m], Zx.v[m]));
+      }
+      if (mey[m]) {
+        Zy.v[m] = A::add(A::mul(be, Zy.v[m]), A::div(A::mul(ce, dxz[m]), p.dx, p.rdx));
+        e1[m] = A::add(e1[m], A::mul(C1.v[m], Zy.v[m]));
+      }
+    }
+    st4(qx, Zx.v);
+    st4(qy, Zy.v);
+  } else if (zmix) {
+    T zx[4], zy[4];
+    int sz[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      int dd = 0;
+      sz[m] = 0;
+      if (qz[m] >= 0) {e_slab(k0 + m, p.kb, p.ke, P, dd, sz[m]);}
+      zx[m] = qz[m] >= 0 && mex[m] ? p.psi[EX][AZ][sz[m]][ob + dz[m]] : T(0);
+      zy[m] = qz[m] >= 0 && mey[m] ? p.psi[EY][AZ][sz[m]][ob + dz[m]] : T(0);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (qz[m] < 0) continue;
+      const T be = p.be[qz[m]], ce = p.ce[qz[m]];
+      if (mex[m]) {
+        zx[m] = A::add(A::mul(be, zx[m]), A::div(A::mul(ce, dyz[m]), p.dx, p.rdx));
+        p.psi[EX][AZ][sz[m]][ob + dz[m]] = zx[m];
+        e0[m] = A::sub(e0[m], A::mul(C0.v[m], zx[m]));
+      }
+      if (mey[m]) {
+        zy[m] = A::add(A::mul(be, zy[m]), A::div(A::mul(ce, dxz[m]), p.dx, p.rdx));
+        p.psi[EY][AZ][sz[m]][ob + dz[m]] = zy[m];
+        e1[m] = A::add(e1[m], A::mul(C1.v[m], zy[m]));
+      }
     }
   }
 #pragma unroll
@@ -398,31 +436,70 @@ __device__ __forceinline__ void v3_edge_h(const Params<T> &p, const VecGeom &g, 
     st4(px, Px.v);
     st4(pz, Pz.v);
   }
-  // update_pml_hx_zinc, update_pml_hy_zinc: old values read before any write
-  int qz[4], dz[4], sz[4];
-  T zx[4], zy[4];
-  const long long ob = ((long long)i * p.ny + j) * P;  // z-slab psi row (i, j)
+  // update_pml_hx_zinc, update_pml_hy_zinc.  The z-slab psi rows are padded to whole four-cell
+  // groups: when the group's slab cells lie on one side (always unless
+  // ke - kb < 2P + 3), its four values are one 16-byte aligned vector of the
+  // row (the rim cells' elements are padding, written back as read);
+  // otherwise cell by cell.
+  int qz[4], dz[4], zside = -1;
+  bool zmix = false;
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
+    int sd = 0;
     dz[m] = 0;
-    sz[m] = 0;
-    qz[m] = mhx[m] || mhy[m] ? h_slab(k0 + m, p.kb, p.ke, P, dz[m], sz[m]) : -1;
-    zx[m] = qz[m] >= 0 && mhx[m] ? p.psi[HX][AZ][sz[m]][ob + dz[m]] : T(0);
-    zy[m] = qz[m] >= 0 && mhy[m] ? p.psi[HY][AZ][sz[m]][ob + dz[m]] : T(0);
-  }
-#pragma unroll
-  for (int m = 0; m < 4; ++m) {
-    if (qz[m] < 0) continue;
-    const T bh = p.bh[qz[m]], ch = p.ch[qz[m]];
-    if (mhx[m]) {
-      zx[m] = A::add(A::mul(bh, zx[m]), A::div(A::mul(ch, dyz[m]), p.dx, p.rdx));
-      p.psi[HX][AZ][sz[m]][ob + dz[m]] = zx[m];
-      h0[m] = A::add(h0[m], A::mul(db, zx[m]));
+    qz[m] = mhx[m] || mhy[m] ? h_slab(k0 + m, p.kb, p.ke, P, dz[m], sd) : -1;
+    if (qz[m] >= 0) {
+      zmix |= zside >= 0 && zside != sd;
+      zside = sd;
     }
-    if (mhy[m]) {
-      zy[m] = A::add(A::mul(bh, zy[m]), A::div(A::mul(ch, dxz[m]), p.dx, p.rdx));
-      p.psi[HY][AZ][sz[m]][ob + dz[m]] = zy[m];
-      h1[m] = A::sub(h1[m], A::mul(db, zy[m]));
+  }
+  const long long ob = ((long long)i * p.ny + j) * p.psz;  // z-slab psi row (i, j)
+  if (zside >= 0 && !zmix) {
+    const int off = k0 - (zside ? p.ke - P : p.kb);  // slab index d of the group's first cell
+    T *const qx = p.psi[HX][AZ][zside] + (ob + off), *const qy = p.psi[HY][AZ][zside] + (ob + off);
+    V4<T> Zx, Zy;
+    ldw4(Zx, qx);
+    ldw4(Zy, qy);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (qz[m] < 0) continue;
+      const T bh = p.bh[qz[m]], ch = p.ch[qz[m]];
+      if (mhx[m]) {
+        Zx.v[m] = A::add(A::mul(bh, Zx.v[m]), A::div(A::mul(ch, dyz[m]), p.dx, p.rdx));
+        h0[m] = A::add(h0[m], A::mul(db, Zx.v[m]));
+      }
+      if (mhy[m]) {
+        Zy.v[m] = A::add(A::mul(bh, Zy.v[m]), A::div(A::mul(ch, dxz[m]), p.dx, p.rdx));
+        h1[m] = A::sub(h1[m], A::mul(db, Zy.v[m]));
+      }
+    }
+    st4(qx, Zx.v);
+    st4(qy, Zy.v);
+  } else if (zmix) {
+    T zx[4], zy[4];
+    int sz[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      int dd = 0;
+      sz[m] = 0;
+      if (qz[m] >= 0) {h_slab(k0 + m, p.kb, p.ke, P, dd, sz[m]);}
+      zx[m] = qz[m] >= 0 && mhx[m] ? p.psi[HX][AZ][sz[m]][ob + dz[m]] : T(0);
+      zy[m] = qz[m] >= 0 && mhy[m] ? p.psi[HY][AZ][sz[m]][ob + dz[m]] : T(0);
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      if (qz[m] < 0) continue;
+      const T bh = p.bh[qz[m]], ch = p.ch[qz[m]];
+      if (mhx[m]) {
+        zx[m] = A::add(A::mul(bh, zx[m]), A::div(A::mul(ch, dyz[m]), p.dx, p.rdx));
+        p.psi[HX][AZ][sz[m]][ob + dz[m]] = zx[m];
+        h0[m] = A::add(h0[m], A::mul(db, zx[m]));
+      }
+      if (mhy[m]) {
+        zy[m] = A::add(A::mul(bh, zy[m]), A::div(A::mul(ch, dxz[m]), p.dx, p.rdx));
+        p.psi[HY][AZ][sz[m]][ob + dz[m]] = zy[m];
+        h1[m] = A::sub(h1[m], A::mul(db, zy[m]));
+      }
     }
   }
 #pragma unroll

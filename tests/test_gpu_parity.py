@@ -92,6 +92,13 @@ def _random_cases():
                                       core_x_nm=100, core_y_nm=120, seed=8),
         "yee3d_p2": lambda: W.strip3d(nx=17, ny=18, nz=35, P=2, src_gap=2, port_gap=4, steps=40, nf=3,
                                       core_x_nm=100, core_y_nm=140, source="TM", seed=9),
+        # z between the rims under 2P + 3 cells: four-cell groups holding cells of both z slabs
+        # (the vector form's padded z-slab rows then take their per-cell path), the source
+        # inside a slab
+        "yee3d_zthin": lambda: W.strip3d(nx=18, ny=17, nz=14, P=4, src_gap=1, port_gap=1, steps=40, nf=3,
+                                         core_x_nm=100, core_y_nm=120, sigma_nm=20, lc_nm=60, seed=12),
+        "yee3d_zthin3": lambda: W.strip3d(nx=18, ny=17, nz=12, P=3, src_gap=1, port_gap=1, steps=40, nf=3,
+                                          core_x_nm=100, core_y_nm=120, source="TM", seed=13),
         # the 2D tile form's shapes: a grid narrower than a halo, and rows longer than a
         # block's threads
         "tm2_narrow": lambda: W.slab2d(nx=14, ny=40, P=2, core_cells=7, src_x=4, ports=(6, 10), steps=40, nf=3),
@@ -137,7 +144,8 @@ def _te2_spec():
                                   "yee3d_p1_wave", "yee3d_p2_wave", "yee3d_graded_wave", "tm2_tile",
                                   "te2_tile", "tm2_p1_tile", "tm2_narrow_tile", "tm2_tall_tile",
                                   "tm2_narrow", "tm2_tall", "tm2_tile2", "te2_tile2", "tm2_p1_tile2",
-                                  "tm2_tile1", "te2_tile1"])
+                                  "tm2_tile1", "te2_tile1", "yee3d_zthin", "yee3d_zthin_cell", "yee3d_zthin_vec",
+                                  "yee3d_zthin_wave", "yee3d_zthin3_vec", "yee3d_zthin3_wave"])
 @pytest.mark.parametrize("ring", [1, 7, 32])
 def test_exact_f64_equals_oracle_random_fields(eng, name, ring):
     base, _, suffix = name.rpartition("_")
