@@ -111,6 +111,42 @@ __device__ __forceinline__ void load_cb(const Params<T> &p, long long bi, int o,
   }
 }
 
+// Prefetch (into L2) of the CPML psi lines a group reads after its curl (its
+// x- and y-slab rows and, in the edge role, its z-slab row), issued before the
+// field loads so that the late loads find the lines on chip.  A prefetch holds
+// no register; the addresses are those the group loads later.  Used by both
+// roles of the H half-step and by the E half-step's edge role: in the E
+// vector role it measured slower on large grids (the 384 x 384 x 256 E
+// half-step 301 against 286 us), elsewhere faster (C2 step 68.1 against
+// 69.8 us).
+__device__ __forceinline__ void prefetch_line(const void *a) { asm volatile("prefetch.global.L2 [%0];" ::"l"(a)); }
+template <typename T, bool HALF_H>
+__device__ __forceinline__ void psi_prefetch(const Params<T> &p, int i, int j, int k0, bool zslab) {
+  constexpr int FX0 = HALF_H ? HY : EY, FX1 = HALF_H ? HZ : EZ, FY0 = HALF_H ? HX : EX, FY1 = HALF_H ? HZ : EZ;
+  constexpr int FZ0 = HALF_H ? HX : EX, FZ1 = HALF_H ? HY : EY;
+  const int P = p.P;
+  int d, side;
+  if ((HALF_H ? h_slab(i, p.ib, p.ie, P, d, side) : e_slab(i, p.ib, p.ie, P, d, side)) >= 0) {
+    const long long oa = ((long long)d * p.ny + j) * p.psx + k0;
+    prefetch_line(p.psi[FX0][AX][side] + oa);
+    prefetch_line(p.psi[FX1][AX][side] + oa);
+  }
+  if ((HALF_H ? h_slab(j, p.jb, p.je, P, d, side) : e_slab(j, p.jb, p.je, P, d, side)) >= 0) {
+    const long long oa = ((long long)i * P + d) * p.psy + k0;
+    prefetch_line(p.psi[FY0][AY][side] + oa);
+    prefetch_line(p.psi[FY1][AY][side] + oa);
+  }
+  if (zslab) {  // the side whose slab cells the group holds (the low one if both)
+    const bool lo = k0 <= p.kb + P - 1 && k0 + 3 >= p.kb, hi = k0 + 3 >= p.ke - P && k0 <= p.ke - 1;
+    if (lo || hi) {
+      const int sd = lo ? LO : HI;
+      const long long oz = ((long long)i * p.ny + j) * p.psz + (k0 - (sd ? p.ke - P : p.kb));
+      prefetch_line(p.psi[FZ0][AZ][sd] + oz);
+      prefetch_line(p.psi[FZ1][AZ][sd] + oz);
+    }
+  }
+}
+
 // Split of a row between the roles (computed on the host per job).
 struct VecGeom {
   int kz0, kz1;  // vector role: k in [kz0, kz1), multiples of 4
@@ -166,6 +202,7 @@ __device__ __forceinline__ void v3_edge_e(const Params<T> &p, const VecGeom &g, 
   const int sy = p.nzp;
   const long long sx = (long long)p.ny * p.nzp, bi = (long long)i * sx;
   const int o = j * sy + k0;
+  psi_prefetch<T, false>(p, i, j, k0, true);
   const T *const hx = p.f[HX] + bi, *const hy = p.f[HY] + bi, *const hz = p.f[HZ] + bi;
   V4<T> Hx, Hy, Hz, Hzy, Hxy, Hzx, Hyx, C0, C1, C2, Ex, Ey, Ez, Rz, Kz;
   ld4(Hx, hx + o);
@@ -358,6 +395,7 @@ __device__ __forceinline__ void v3_edge_h(const Params<T> &p, const VecGeom &g, 
   const int sy = p.nzp;
   const long long sx = (long long)p.ny * p.nzp, bi = (long long)i * sx;
   const int o = j * sy + k0;
+  psi_prefetch<T, true>(p, i, j, k0, true);
   const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
   V4<T> Ex, Ey, Ez, Ezy, Exy, Ezx, Eyx, Hx, Hy, Hz, Rz, Kz;
   ld4e<CG>(Ex, ex + o);
@@ -689,6 +727,7 @@ __device__ __forceinline__ void v3_h_block(const Params<T> &p, const VecGeom &g,
   const int sy = p.nzp;
   const long long sx = (long long)p.ny * p.nzp, bi = (long long)i * sx;
   const int o = j * sy + k0;
+  psi_prefetch<T, true>(p, i, j, k0, false);
   const T *const ex = p.f[EX] + bi, *const ey = p.f[EY] + bi, *const ez = p.f[EZ] + bi;
   V4<T> Ex, Ey, Ez, Ezy, Exy, Ezx, Eyx, Hx, Hy, Hz, Rz, Kz;
   ld4e<CG>(Ex, ex + o);
