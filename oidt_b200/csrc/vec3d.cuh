@@ -15,8 +15,8 @@
 //   four-cell group) pairs, so no lane idles whatever nz is.
 // * edge role: every other four-cell group (the z slabs, the rim and the row
 //   padding: 9 % of the cells of a 256-cell guide with a 10-cell CPML), with
-//   each component's update range tested per cell and the z-slab psi read and
-//   written per cell.
+//   each component's update range tested per cell and the z-slab psi moved
+//   per group in rows padded to whole groups.
 //
 // Per cell the arithmetic is the sequence of kernels.cuh's y3_e_compute /
 // y3_h_compute (the reference's fdtd_funcs.py:43-266 in its launch order):
@@ -164,9 +164,10 @@ template <typename T> __device__ __forceinline__ bool near_src(const Params<T> &
 
 // Edge role: four-cell groups k0 in [0, kz0) and [kz1, nzp) -- the z slabs,
 // the rim and the row padding -- with the update range of every component
-// tested per cell and the z-slab psi read and written per cell (all old
-// values of a group read before the first write).  Groups within one cell of
-// the source box run y3_e_cell / y3_h_cell per cell.
+// tested per cell.  A group's z-slab psi values are one 16-byte vector of the
+// padded z-slab rows, unless the group holds cells of both z slabs (then cell
+// by cell); all old values of a group are read before the first write.
+// Groups within one cell of the source box run y3_e_cell / y3_h_cell per cell.
 template <typename T>
 __device__ __forceinline__ bool edge_group(const Params<T> &p, const VecGeom &g, int bx, int &j, int &k0) {
   const int nge = g.nedge >> 2;
