@@ -122,3 +122,30 @@ def test_tuning_needs_enough_steps():
     t = tune.Tuner(eng=None, reps=3)
     with pytest.raises(ValueError):
         t.time_choice(_strip(steps=100), dict(tune.DEFAULT), np.float32, ring_steps=32)
+
+
+@pytest.mark.parametrize("nx,ny,nz,P", [(20, 19, 40, 4), (22, 18, 64, 3), (16, 15, 32, 1), (30, 44, 128, 10)])
+@pytest.mark.parametrize("prec", [np.float32, np.float64])
+def test_vector_form_pads_z_slab_rows_to_whole_groups(nx, ny, nz, P, prec):
+    """The vector form's z-slab psi rows hold every four-cell group that meets
+    the slab: slab cell d of the low side at k - floor4(kb), of the high side
+    at k - floor4(ke - P), rows of the larger span rounded up to 4.  With nz a
+    multiple of 4 (x- and y-slab rows then as long as the reference's), the
+    form needs exactly those eight arrays' extra bytes over the per-cell form
+    (256-byte aligned sub-buffers)."""
+    from oidt_b200.engine import load_library
+    from oidt_b200.spec import to_desc
+    lib = load_library()
+    spec = _strip(nx=nx, ny=ny, nz=nz, P=P, steps=50)
+    kb, ke = spec.lim_lo[2], spec.lim_hi[2]
+    zoff = (kb - kb // 4 * 4, (ke - P) - (ke - P) // 4 * 4)
+    psz = (max(zoff) + P + 3) // 4 * 4
+    esz = np.dtype(prec).itemsize
+    al = lambda x: (x + 255) // 256 * 256  # noqa: E731
+    sizes = {}
+    for v in ("vec", "cell"):
+        d, keep = to_desc(spec, variant=v, precision=prec)
+        rc, sizes[v] = _bytes(lib, d)
+        assert rc == 0
+    # E: Ex, Ey; H: Hx, Hy; two sides each
+    assert sizes["vec"] - sizes["cell"] == 8 * (al(nx * ny * psz * esz) - al(nx * ny * P * esz))
